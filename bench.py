@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 tree pipeline (7 stages, bit-exact): points/sec.
+
+Default workload: the plain pipeline at scale, n = 16,777,216 points uniform
+in [0, 1024)^3, 32-bit Morton keys, one cloud per GPU ("replicas only": the
+path does not shard; with --gpus N every rank builds its own cloud's octree).
+
+  value    - points/s with the points already in HBM: K back-to-back runs of
+             the fused pipeline (rw_tree_pipeline_enqueue), CUDA events on the
+             launching stream, max over ranks.
+  e2e      - the same metric through rw_tree_run_host with pinned host
+             buffers: H2D of the points, the pipeline, D2H of the counts and
+             the octree rows, every step.
+  roofline - the dominant kernel's algorithmic bytes per launch / its mean
+             CUDA-event duration inside the pipeline, against the measured
+             HBM copy bandwidth.
+  cpu_baseline - the reference's own CPU path (cpu::run_stage1..7 compiled
+             from its sources, oracle/_ref) on all host cores, rank 0, N = 1.
+
+`--impl reference` times only the reference's CPU path on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "octree-build points/sec (7 stages, bit-exact): plain vs batched/learned, 1 B200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--n", type=int, default=16777216)
+    p.add_argument("--dist", choices=("uniform", "gauss", "appdata"), default="uniform")
+    p.add_argument("--key-bits", type=int, default=32, choices=(32, 64))
+    p.add_argument("--radix-bits", type=int, default=0, choices=(0, 8, 11))
+    p.add_argument("--seed", type=int, default=20260101)
+    p.add_argument("--no-verify", action="store_true", help="skip the oracle check")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_points(rw, n, dist, seed):
+    if dist == "appdata":
+        return rw.generate_points(n, rw.GEN_APPDATA, 114514)
+    if dist == "uniform":
+        return rw.generate_points(n, rw.GEN_UNIFORM, seed)
+    return rw.generate_points(n, rw.GEN_GAUSSIAN_MIXTURE, seed, n_components=32,
+                              sigma_lo=4.0, sigma_hi=40.0)
+
+
+def workload_name(a):
+    d = {"uniform": "uniform [0,1024)^3", "gauss": "32-component Gaussian mixture sigma 4-40",
+         "appdata": "AppData mt19937(114514) uniform"}[a.dist]
+    return f"plain tree pipeline (7 stages), n={a.n:,} points, {d}, {a.key_bits}-bit Morton"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is None:
+            return False
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def kernel_bytes(name, n, u, m, K):
+    """Algorithmic bytes of one launch (each input read once, each output
+    written once; neighbour reads counted as cache hits)."""
+    b = max(u - 1, 0)
+    if name == "morton_histogram":
+        return (16 + K) * n
+    if name.startswith("sort_pass"):
+        return 2 * K * n
+    if name == "unique":
+        return K * n + K * u
+    if name == "radix_tree_edges_scan":
+        # codes read; prefix_n, 2 leaf flags, left_child, parent, edge count, offset written
+        return K * u + 19 * b
+    if name == "octree_rows":
+        # codes, prefix_n, count, offset read; corner 16 + cell 4 + children 32 + masks 8 written
+        return (K + 9) * b + 60 * m
+    if name == "octree_links":
+        # count, parent, offset, codes, prefix_n read; one child slot and one mask per link
+        return (K + 13) * b + 8 * m
+    return 0
+
+
+def pipeline_bytes(n, u, m, K, passes):
+    """Whole-pipeline algorithmic bytes (per-stage formulas: S1 (16+K)n,
+    S2 K n (1+2P), S3 K(n+u), S4 K u + 11 b, S5 10 b, S6 8 b,
+    S7 (13+K) b + 72 m)."""
+    b = u - 1
+    return ((16 + K) * n + K * n * (1 + 2 * passes) + K * (n + u) + K * u + 11 * b
+            + 10 * b + 8 * b + (13 + K) * b + 72 * m)
+
+
+def traffic_table():
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return 0
+    from oracle import RefTree, ref_available
+    from __graft_entry__ import _load_package
+    rw = _load_package()
+    pts = make_points(rw, a.n, a.dist, a.seed)
+    if a.key_bits != 32 or not ref_available():
+        # the reference has no 64-bit path; the C restatement stands in
+        from oracle import Oracle
+        orc = Oracle()
+        kind, cores = "port", 1
+        for _ in range(a.warmup):
+            orc.run(pts, key_bits=a.key_bits)
+        ms = []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            orc.run(pts, key_bits=a.key_bits)
+            ms.append((time.perf_counter() - t0) * 1e3)
+    else:
+        ref = RefTree()
+        cores = ref.hardware_threads()
+        kind = "reference"
+        ms = list(ref.time(pts, cores, a.warmup + a.steps))[a.warmup:]
+    t = statistics.median(ms)
+    val = a.n / (t / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "points/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": f"u{a.key_bits}", "data": "synthetic",
+        "config": {"workload": workload_name(a), "n_points": a.n,
+                   "l2": "inputs larger than L2 (points 16 B each)"},
+        "cpu_baseline": {"value": val, "unit": "points/s", "cores": cores, "kind": kind,
+                         "sample": f"{a.steps} full runs of stages 1-7 on the n={a.n} cloud, "
+                                   f"median wall time"},
+        "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(rw, pts, a):
+    from oracle import RefTree, ref_available
+    if a.key_bits != 32 or not ref_available():
+        from oracle import Oracle
+        orc = Oracle()
+        t0 = time.perf_counter()
+        orc.run(pts, key_bits=a.key_bits)
+        t = time.perf_counter() - t0
+        return {"value": a.n / t, "unit": "points/s", "cores": 1, "kind": "port",
+                "sample": f"1 run of the C restatement on the n={a.n} cloud"}
+    ref = RefTree()
+    cores = ref.hardware_threads()
+    first = ref.time(pts, cores, 1)[0]
+    iters = int(min(10, max(3, 15000.0 / max(first, 1.0))))
+    ms = ref.time(pts, cores, iters)
+    t = statistics.median(ms)
+    return {"value": a.n / (t / 1e3), "unit": "points/s", "cores": cores, "kind": "reference",
+            "sample": f"median of {iters} runs of cpu::run_stage1..7 (verbatim, "
+                      f"{cores} threads) on the same n={a.n} cloud, after 1 warm run"}
+
+
+def main():
+    a = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a, rank)
+
+    import torch
+    import torch.distributed as dist
+    from __graft_entry__ import _load_package
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    rw = _load_package()
+    K = 4 if a.key_bits == 32 else 8
+
+    pts = make_points(rw, a.n, a.dist, a.seed + rank)
+    app = rw.AppData(a.n, a.key_bits, points=pts)
+    im = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
+    passes = -(-(30 if a.key_bits == 32 else 63) // (a.radix_bits or 8))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.current_stream()
+    for _ in range(a.warmup):
+        rw.run_pipeline(app, im)
+    u, m = app.get_n_unique(), app.get_n_octree_nodes()
+
+    mismatches = None
+    if not a.no_verify and rank == 0:
+        from oracle import Oracle
+        want = Oracle().run(pts, key_bits=a.key_bits).trimmed()
+        got = app.results()
+        mismatches = sum(
+            1 for k, v in want.items()
+            if (np.ascontiguousarray(got[k]).tobytes() != np.ascontiguousarray(v).tobytes()
+                if isinstance(v, np.ndarray) else got[k] != v))
+
+    # ---- device-resident timed region ------------------------------------
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            rw.pipeline_enqueue(app, im)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    rw.pipeline_finish(app, im)
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1) / a.steps)
+    value = a.n * world / (ms_step / 1e3)
+
+    # ---- per-kernel device times inside the pipeline -----------------------
+    kms = rw.profile_pipeline(app, im, reps=max(3, min(10, a.steps)))
+    hbm, peak_kind = peaks()
+    stages = {}
+    for name, t in kms.items():
+        by = kernel_bytes(name, a.n, u, m, K)
+        gbs = by / (t * 1e-3) / 1e9 if t > 0 and by else None
+        stages[name] = {"ms": round(t, 5), "bytes": by,
+                        "gbs": round(gbs, 1) if gbs else None,
+                        "frac": round(gbs / hbm, 3) if gbs else None}
+    dom = max(kms, key=kms.get)
+    tt = traffic_table()
+    dom_traffic = None
+    key = f"{a.dist}-{a.key_bits}-{dom}"
+    if key in tt:
+        dom_traffic = tt[key]
+    dom_gbs = stages[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": round(dom_gbs / hbm, 4) if dom_gbs else None,
+                "traffic": dom_traffic, "peak_source": f"{peak_kind} hbm_gbs"}
+    pipe_b = pipeline_bytes(a.n, u, m, K, passes)
+    pipe_gbs = pipe_b / (ms_step * 1e-3) / 1e9
+
+    # ---- end to end through the host-facing C ABI call ---------------------
+    h_pts = torch.from_numpy(pts).pin_memory()
+    cap = rw.octree_capacity(a.n)
+    outs = {
+        "children": torch.empty((cap, 8), dtype=torch.int32).pin_memory(),
+        "corner": torch.empty((cap, 4), dtype=torch.float32).pin_memory(),
+        "cell_size": torch.empty(cap, dtype=torch.float32).pin_memory(),
+        "child_node_mask": torch.empty(cap, dtype=torch.int32).pin_memory(),
+        "child_leaf_mask": torch.empty(cap, dtype=torch.int32).pin_memory(),
+    }
+    outs_np = {k: v.numpy() for k, v in outs.items()}
+    h_np = h_pts.numpy()
+    for _ in range(2):
+        rw.run_host(app, im, h_np, outs_np)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, min(a.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        rw.run_host(app, im, h_np, outs_np)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    m2 = app.get_n_octree_nodes()
+    d2h = 60 * m2 + 16
+    e2e = {"value": a.n * world / (e2e_ms / 1e3), "unit": "points/s",
+           "h2d_bytes_per_step": 16 * a.n, "d2h_bytes_per_step": d2h,
+           "ms_per_step": round(e2e_ms, 4),
+           "path": "rw_tree_run_host: pinned host points -> H2D -> 7 stages -> counts + "
+                   "octree rows (children, corner, cell_size, masks) D2H"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(rw, pts, a)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": f"u{a.key_bits}", "data": "synthetic",
+        "config": {"workload": workload_name(a), "n_points": a.n, "key_bits": a.key_bits,
+                   "radix_bits": a.radix_bits or 8, "sort_passes": passes,
+                   "parallelism": f"replicas x{world} (one cloud per GPU)",
+                   "l2": "inputs larger than L2 (points 268 MB per step)"},
+        "n_unique": u, "n_octree_nodes": m, "mismatches_vs_oracle": mismatches,
+        "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
+                              "frac": round(pipe_gbs / hbm, 4)},
+        "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
+        "clocks": clocks.summary(), "gpu_launches": (6 + passes) * a.steps,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,215 @@
+/* rw_tree.h - C ABI of the B200 tree pipeline (point cloud -> octree).
+ *
+ * Drop-in for the CUDA path of ucsc-redwood/redwood-comp's tree app.  Every
+ * entry point takes plain pointers and sizes.  The reference interfaces each
+ * one replaces are cited beside it (paths inside the reference project).
+ *
+ * Buffers: `rw_tree_app_data` mirrors the reference's `AppData`
+ * (apps/tree/app_data.hpp:15-158) field by field; the caller owns every buffer
+ * (device or managed memory, as the reference's pmr memory resource decides,
+ * redwood/cuda/cu_mem_resource.cu:9-27).  Scratch lives in an
+ * `rw_tree_im_storage` (the reference's `cuda::ImStorage`,
+ * apps/tree/cuda/im_storage.cuh:10-42), allocated by the library.
+ *
+ * Buffer contract (app_data.hpp:139-157): stage 2 leaves the sorted keys in
+ * u_morton_keys_alt, stage 3 leaves the unique keys in u_morton_keys.
+ *
+ * Errors: every call returns RW_OK (0) or an rw_status code; the C++ layer in
+ * redwood_tree/ turns a non-zero code into std::runtime_error as the
+ * reference's CUDA_CHECK does (redwood/cuda/helpers.cuh:12-20).
+ */
+#ifndef RW_TREE_H
+#define RW_TREE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same type as cudaStream_t (CUstream_st*), declared here so that callers
+ * need no CUDA headers.  NULL is the legacy default stream. */
+typedef struct CUstream_st* rw_stream_t;
+
+typedef enum rw_status {
+  RW_OK = 0,
+  RW_ERR_ARG = 1,        /* null pointer, n out of range, bad key width */
+  RW_ERR_DEGENERATE = 2, /* fewer than 3 distinct keys: the reference's root
+                            range [0, n_brt-1] (func_brt.hpp:80-83) is empty */
+  RW_ERR_CAPACITY = 3,   /* n_octree_nodes + 1 exceeds the octree rows
+                            (AppData allocates floor(0.6 n), app_data.hpp:28) */
+  RW_ERR_CUDA = 4,       /* a CUDA runtime call failed (rw_tree_last_error) */
+  RW_ERR_TIMEOUT = 5,    /* a device-side bounded wait gave up */
+  RW_ERR_NOT_READY = 6,  /* a stage ran before the stage that sets its count */
+  RW_ERR_NO_DEVICE = 7   /* no usable CUDA device / kernel image */
+} rw_status;
+
+#define RW_COUNT_UNSET 0xffffffffu
+/* Largest point count: look-back descriptors carry 30-bit values. */
+#define RW_MAX_POINTS ((uint32_t)1 << 30)
+
+/* Mirror of AppData (app_data.hpp:15-96).  Counts start at RW_COUNT_UNSET
+ * (the reference's numeric_limits<uint32_t>::max(), :49-51) and are set by
+ * stages 3 and 6.  Keys are uint32_t (key_bits 32: 10 bits per axis, the
+ * reference) or uint64_t (key_bits 64: 21 bits per axis, no reference
+ * counterpart). */
+typedef struct rw_tree_app_data {
+  uint32_t n_input;
+  uint32_t oct_capacity; /* rows of every oct_* buffer */
+  int32_t key_bits;      /* 32 or 64 */
+  float min_coord;       /* AppData::min_coord (0.0f) */
+  float range;           /* AppData::range (1024.0f) */
+  uint32_t n_unique;
+  uint32_t n_brt_nodes;
+  uint32_t n_octree_nodes;
+  float* u_input_points;      /* [4 n] x y z w (glm::vec4) */
+  void* u_morton_keys;        /* [n] */
+  void* u_morton_keys_alt;    /* [n] */
+  int32_t* u_edge_count;      /* [n] */
+  int32_t* u_edge_offset;     /* [n] */
+  uint8_t* brt_prefix_n;      /* [n] RadixTree (app_data.hpp:63-76) */
+  uint8_t* brt_has_leaf_left; /* [n] */
+  uint8_t* brt_has_leaf_right;/* [n] */
+  int32_t* brt_left_child;    /* [n] */
+  int32_t* brt_parents;       /* [n] */
+  int32_t* oct_children;      /* [8 cap] Octree (app_data.hpp:78-96) */
+  float* oct_corner;          /* [4 cap] */
+  float* oct_cell_size;       /* [cap] */
+  int32_t* oct_child_node_mask; /* [cap] */
+  int32_t* oct_child_leaf_mask; /* [cap] stays 0: the reference never links
+                                   leaves (cu_dispatcher.cu:738-749) */
+} rw_tree_app_data;
+
+/* Opaque scratch: sort histograms and look-back descriptors, the ping-pong
+ * key buffer, device-side counts and the error word. */
+typedef struct rw_tree_im_storage rw_tree_im_storage;
+
+/* Octree rows for n points: floor(n * 0.6f) in float (app_data.hpp:13,28). */
+uint32_t rw_tree_octree_capacity(uint32_t n_input);
+
+/* Fills `app` for n points: counts unset, min 0, range 1024, buffers NULL. */
+void rw_tree_app_data_init(rw_tree_app_data* app, uint32_t n_input,
+                           int32_t key_bits);
+
+/* ImStorage(int n) (im_storage.cuh:11, im_storage.cu:29-40): allocates the
+ * scratch for up to n_input points on the current device. */
+int rw_tree_im_storage_create(uint32_t n_input, int32_t key_bits,
+                              rw_tree_im_storage** out);
+/* Same, with the sort's digit width chosen: 8 or 11 bits (0 = default 8).
+ * The reference fixes 8-bit digits (cu_dispatcher.cu:25-27). */
+int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
+                                 int32_t radix_bits, rw_tree_im_storage** out);
+/* ~ImStorage (im_storage.cu:42-52). */
+int rw_tree_im_storage_destroy(rw_tree_im_storage* im);
+/* ImStorage::clearSmem (im_storage.cu:53-60): zeroes histograms, descriptors
+ * and the error word on `stream`.  The stage calls do this themselves. */
+int rw_tree_im_storage_clear(rw_tree_im_storage* im, rw_stream_t stream);
+
+/* cuda::run_stage1..7 (apps/tree/cuda/cu_dispatcher.cuh:8-19,
+ * cu_dispatcher.cu:501-752).  Synchronous like the reference: each call ends
+ * with a stream synchronisation and updates the counts in `app`.  The
+ * reference passes ImStorage to stages 2 and 3 only; here every stage takes it
+ * (the C++ layer supplies an internal one where the reference signature has
+ * none).
+ *   1: u_input_points -> u_morton_keys                         (01_morton.cu)
+ *   2: u_morton_keys -> u_morton_keys_alt, ascending          (onesweep sort)
+ *   3: u_morton_keys_alt -> u_morton_keys unique, n_unique    (03_unique.cu)
+ *   4: unique keys -> brt_* for i in [0, n_brt)             (04_radix_tree.cu)
+ *   5: brt -> u_edge_count                                 (05_edge_count.cu)
+ *   6: u_edge_count -> u_edge_offset (exclusive), n_octree_nodes
+ *                                                         (06_prefix_sum.cu)
+ *   7: everything -> oct_* rows [0, n_octree_nodes)          (07_octree.cu) */
+int rw_tree_run_stage1(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage2(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage3(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage4(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage5(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage6(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+int rw_tree_run_stage7(rw_tree_app_data* app, rw_tree_im_storage* im,
+                       rw_stream_t stream);
+
+/* All seven stages as one asynchronous sequence on `stream` (the loop body of
+ * pipe_main_baseline.cpp:55-92 without its per-stage host synchronisations):
+ * fused kernels, counts kept on the device, no host round trip.  Capturable
+ * into a CUDA graph.  Outputs are identical to stages 1..7 run one by one.
+ * rw_tree_pipeline_finish waits for the stream, copies the counts into `app`
+ * and reports any device-side error. */
+int rw_tree_pipeline_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im,
+                             rw_stream_t stream);
+int rw_tree_pipeline_finish(rw_tree_app_data* app, rw_tree_im_storage* im,
+                            rw_stream_t stream);
+
+/* Per-kernel device times of the fused pipeline, the role of the reference's
+ * per-stage google-benchmark fixtures (apps/tree/bm_cuda.cpp:25-123): runs
+ * the pipeline `reps` times with a CUDA event after every kernel and writes
+ * the mean milliseconds of each kernel to kernel_ms (order and names as in
+ * rw_tree_pipeline_kernel_names, comma separated). */
+int rw_tree_pipeline_profile(rw_tree_app_data* app, rw_tree_im_storage* im,
+                             rw_stream_t stream, int32_t reps, float* kernel_ms,
+                             int32_t max_kernels, int32_t* n_kernels);
+const char* rw_tree_pipeline_kernel_names(const rw_tree_im_storage* im);
+
+/* Host-side result buffers for rw_tree_run_host; any pointer may be NULL. */
+typedef struct rw_tree_host_out {
+  void* sorted_keys;          /* [n] */
+  void* unique_keys;          /* [n_unique] */
+  uint8_t* prefix_n;          /* [n_brt] */
+  uint8_t* has_leaf_left;
+  uint8_t* has_leaf_right;
+  int32_t* left_child;
+  int32_t* parents;
+  int32_t* edge_count;
+  int32_t* edge_offset;
+  int32_t* children;          /* [8 n_octree_nodes] */
+  float* corner;              /* [4 n_octree_nodes] */
+  float* cell_size;           /* [n_octree_nodes] */
+  int32_t* child_node_mask;
+  int32_t* child_leaf_mask;
+} rw_tree_host_out;
+
+/* End to end from host memory, the way the reference's callers use managed
+ * AppData (apps/tree/main.cpp:48-88): copies h_points ([4 n] floats) into
+ * app->u_input_points, runs the pipeline, reads the counts and copies the
+ * requested outputs back.  Pinned host buffers give full PCIe bandwidth. */
+int rw_tree_run_host(rw_tree_app_data* app, rw_tree_im_storage* im,
+                     const float* h_points, rw_tree_host_out* h_out,
+                     rw_stream_t stream);
+
+/* Seeded synthetic point clouds, generated on the host.
+ *   RW_GEN_APPDATA: AppData's own generator (app_data.hpp:32-39):
+ *     std::mt19937(seed), uniform_real_distribution<float>(min, min+range),
+ *     w = 1.  The reference writes glm::vec4(dis(gen), dis(gen), dis(gen), 1)
+ *     whose argument order C++ leaves unspecified; g++ builds of it draw z,
+ *     then y, then x, and so does this generator.
+ *   RW_GEN_UNIFORM: counter-based (splitmix64) uniform in [min, min+range).
+ *   RW_GEN_GAUSSIAN_MIXTURE: counter-based isotropic Gaussian mixture with
+ *     n_components centres uniform in the box, sigma uniform in
+ *     [sigma_lo, sigma_hi], equal weights, clamped into the box. */
+typedef enum rw_gen_kind {
+  RW_GEN_APPDATA = 0,
+  RW_GEN_UNIFORM = 1,
+  RW_GEN_GAUSSIAN_MIXTURE = 2
+} rw_gen_kind;
+
+int rw_tree_generate_points(float* out, uint64_t n, int32_t kind,
+                            uint64_t seed, float min_coord, float range,
+                            int32_t n_components, float sigma_lo,
+                            float sigma_hi);
+
+/* Text of the last CUDA error seen by this thread ("" if none). */
+const char* rw_tree_last_error(void);
+/* Library build tag (kernels compiled for sm_100a). */
+const char* rw_tree_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RW_TREE_H */

@@ -1,0 +1,334 @@
+"""Python host side of the B200 tree pipeline, over the C ABI of rw_tree.h.
+
+Mirrors the reference's tree-app surface (ucsc-redwood/redwood-comp,
+apps/tree): ``AppData`` with the same buffer names (app_data.hpp:15-158),
+``ImStorage`` (cuda/im_storage.cuh:10-42) and ``run_stage1..7``
+(cuda/cu_dispatcher.cuh:8-19), plus ``run_pipeline`` (all seven stages fused,
+counts on the device) and ``run_host`` (end to end from host memory).
+
+PyTorch only provides device memory and the current stream.  Every stage runs
+in the sm_100a kernels of librw_tree.so; there is no CPU fallback, and loading
+fails loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+__all__ = [
+    "RwTreeError", "lib", "AppData", "ImStorage", "run_stage1", "run_stage2",
+    "run_stage3", "run_stage4", "run_stage5", "run_stage6", "run_stage7",
+    "run_pipeline", "run_host", "generate_points", "octree_capacity",
+    "GEN_APPDATA", "GEN_UNIFORM", "GEN_GAUSSIAN_MIXTURE", "COUNT_UNSET",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librw_tree.so")
+
+RW_OK, RW_ERR_ARG, RW_ERR_DEGENERATE, RW_ERR_CAPACITY = 0, 1, 2, 3
+RW_ERR_CUDA, RW_ERR_TIMEOUT, RW_ERR_NOT_READY, RW_ERR_NO_DEVICE = 4, 5, 6, 7
+STATUS_NAMES = {
+    0: "RW_OK", 1: "RW_ERR_ARG", 2: "RW_ERR_DEGENERATE", 3: "RW_ERR_CAPACITY",
+    4: "RW_ERR_CUDA", 5: "RW_ERR_TIMEOUT", 6: "RW_ERR_NOT_READY",
+    7: "RW_ERR_NO_DEVICE",
+}
+COUNT_UNSET = 0xFFFFFFFF
+GEN_APPDATA, GEN_UNIFORM, GEN_GAUSSIAN_MIXTURE = 0, 1, 2
+DEFAULT_SEED = 114514  # app_data.hpp:32
+
+_vp = ctypes.c_void_p
+
+
+class RwTreeError(RuntimeError):
+    """A non-zero rw_status (the reference throws std::runtime_error from
+    CUDA_CHECK and from unset-count getters, redwood/cuda/helpers.cuh:12-20,
+    app_data.hpp:110-133)."""
+
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        msg = f"{where}: {STATUS_NAMES.get(code, code)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+class _AppDataC(ctypes.Structure):
+    _fields_ = [
+        ("n_input", ctypes.c_uint32), ("oct_capacity", ctypes.c_uint32),
+        ("key_bits", ctypes.c_int32), ("min_coord", ctypes.c_float),
+        ("range", ctypes.c_float), ("n_unique", ctypes.c_uint32),
+        ("n_brt_nodes", ctypes.c_uint32), ("n_octree_nodes", ctypes.c_uint32),
+        ("u_input_points", _vp), ("u_morton_keys", _vp), ("u_morton_keys_alt", _vp),
+        ("u_edge_count", _vp), ("u_edge_offset", _vp), ("brt_prefix_n", _vp),
+        ("brt_has_leaf_left", _vp), ("brt_has_leaf_right", _vp),
+        ("brt_left_child", _vp), ("brt_parents", _vp), ("oct_children", _vp),
+        ("oct_corner", _vp), ("oct_cell_size", _vp), ("oct_child_node_mask", _vp),
+        ("oct_child_leaf_mask", _vp),
+    ]
+
+
+class _HostOutC(ctypes.Structure):
+    _fields_ = [(name, _vp) for name in (
+        "sorted_keys", "unique_keys", "prefix_n", "has_leaf_left", "has_leaf_right",
+        "left_child", "parents", "edge_count", "edge_offset", "children", "corner",
+        "cell_size", "child_node_mask", "child_leaf_mask")]
+
+
+_LIB = None
+
+EXPORTS = (
+    "rw_tree_octree_capacity", "rw_tree_app_data_init", "rw_tree_im_storage_create",
+    "rw_tree_im_storage_create_ex", "rw_tree_im_storage_destroy",
+    "rw_tree_im_storage_clear", "rw_tree_run_stage1", "rw_tree_run_stage2",
+    "rw_tree_run_stage3", "rw_tree_run_stage4", "rw_tree_run_stage5",
+    "rw_tree_run_stage6", "rw_tree_run_stage7", "rw_tree_pipeline_enqueue",
+    "rw_tree_pipeline_finish", "rw_tree_run_host", "rw_tree_generate_points",
+    "rw_tree_last_error", "rw_tree_version", "rw_tree_pipeline_profile",
+    "rw_tree_pipeline_kernel_names",
+)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded librw_tree.so (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with "
+                               "`make -C redwood-comp_b200` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.rw_tree_octree_capacity.restype = ctypes.c_uint32
+        L.rw_tree_octree_capacity.argtypes = [ctypes.c_uint32]
+        L.rw_tree_app_data_init.restype = None
+        L.rw_tree_last_error.restype = ctypes.c_char_p
+        L.rw_tree_version.restype = ctypes.c_char_p
+        L.rw_tree_pipeline_kernel_names.restype = ctypes.c_char_p
+        L.rw_tree_generate_points.argtypes = [
+            _vp, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_float,
+            ctypes.c_float, ctypes.c_int32, ctypes.c_float, ctypes.c_float]
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != RW_OK:
+        raise RwTreeError(rc, where, lib().rw_tree_last_error().decode())
+
+
+def octree_capacity(n: int) -> int:
+    return int(lib().rw_tree_octree_capacity(n))
+
+
+def generate_points(n: int, kind: int = GEN_APPDATA, seed: int = DEFAULT_SEED,
+                    min_coord: float = 0.0, range_: float = 1024.0,
+                    n_components: int = 32, sigma_lo: float = 4.0,
+                    sigma_hi: float = 40.0, out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Seeded [n, 4] float32 points (host memory); see rw_tree_generate_points."""
+    pts = out if out is not None else np.empty((n, 4), np.float32)
+    assert pts.dtype == np.float32 and pts.shape == (n, 4) and pts.flags.c_contiguous
+    _check(lib().rw_tree_generate_points(
+        pts.ctypes.data_as(_vp), n, kind, seed, min_coord, range_, n_components,
+        sigma_lo, sigma_hi), "generate_points")
+    return pts
+
+
+def _stream_handle(stream) -> _vp:
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return _vp(s.cuda_stream)
+
+
+class ImStorage:
+    """Scratch of one pipeline (the reference's cuda::ImStorage)."""
+
+    def __init__(self, n_input: int, key_bits: int = 32, radix_bits: int = 0):
+        self._h = _vp()
+        _check(lib().rw_tree_im_storage_create_ex(
+            ctypes.c_uint32(n_input), ctypes.c_int32(key_bits), ctypes.c_int32(radix_bits),
+            ctypes.byref(self._h)), "ImStorage")
+        self.n_input, self.key_bits, self.radix_bits = n_input, key_bits, radix_bits
+
+    @property
+    def handle(self) -> _vp:
+        return self._h
+
+    def clear(self, stream=None) -> None:
+        _check(lib().rw_tree_im_storage_clear(self._h, _stream_handle(stream)), "clearSmem")
+
+    def close(self) -> None:
+        if self._h:
+            lib().rw_tree_im_storage_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class AppData:
+    """Device-resident buffers of one point cloud, named as in AppData.
+
+    ``points``: [n, 4] float32 host array; by default the reference's own
+    seeded input (mt19937(114514) uniform in [0, 1024), app_data.hpp:32-39).
+    """
+
+    min_coord = 0.0
+    range = 1024.0
+
+    def __init__(self, n_input: int, key_bits: int = 32,
+                 points: Optional[np.ndarray] = None, device: str = "cuda",
+                 min_coord: float = 0.0, range_: float = 1024.0):
+        import torch
+        if key_bits not in (32, 64):
+            raise ValueError("key_bits must be 32 or 64")
+        self.n_input = n = int(n_input)
+        self.key_bits = key_bits
+        self.min_coord, self.range = float(min_coord), float(range_)
+        self.oct_capacity = cap = octree_capacity(n)
+        kt = torch.int32 if key_bits == 32 else torch.int64
+        dev = torch.device(device)
+        e = lambda *shape, dtype: torch.zeros(*shape, dtype=dtype, device=dev)
+        self.u_input_points = e(n, 4, dtype=torch.float32)
+        self.u_morton_keys = e(n, dtype=kt)
+        self.u_morton_keys_alt = e(n, dtype=kt)
+        self.u_edge_count = e(n, dtype=torch.int32)
+        self.u_edge_offset = e(n, dtype=torch.int32)
+        self.brt_prefix_n = e(n, dtype=torch.uint8)
+        self.brt_has_leaf_left = e(n, dtype=torch.uint8)
+        self.brt_has_leaf_right = e(n, dtype=torch.uint8)
+        self.brt_left_child = e(n, dtype=torch.int32)
+        self.brt_parents = e(n, dtype=torch.int32)
+        rows = max(cap, 1)
+        self.oct_children = e(rows, 8, dtype=torch.int32)
+        self.oct_corner = e(rows, 4, dtype=torch.float32)
+        self.oct_cell_size = e(rows, dtype=torch.float32)
+        self.oct_child_node_mask = e(rows, dtype=torch.int32)
+        self.oct_child_leaf_mask = e(rows, dtype=torch.int32)
+        if points is None:
+            points = generate_points(n, GEN_APPDATA, DEFAULT_SEED, min_coord, range_)
+        self.set_points(points)
+        c = _AppDataC()
+        lib().rw_tree_app_data_init(ctypes.byref(c), ctypes.c_uint32(n), ctypes.c_int32(key_bits))
+        c.min_coord, c.range = self.min_coord, self.range
+        for name, _ in _AppDataC._fields_:
+            if hasattr(self, name) and name.startswith(("u_", "brt_", "oct_")) and name != "oct_capacity":
+                setattr(c, name, getattr(self, name).data_ptr())
+        self._c = c
+
+    # -- data movement ------------------------------------------------------
+    def set_points(self, points: np.ndarray) -> None:
+        import torch
+        pts = np.ascontiguousarray(points, np.float32).reshape(self.n_input, 4)
+        self.u_input_points.copy_(torch.from_numpy(pts))
+
+    @property
+    def c(self) -> _AppDataC:
+        return self._c
+
+    # -- counts (app_data.hpp:108-137) ---------------------------------------
+    def get_n_input(self) -> int:
+        return self.n_input
+
+    def get_n_unique(self) -> int:
+        if self._c.n_unique == COUNT_UNSET:
+            raise RuntimeError("n_unique is not set")
+        return int(self._c.n_unique)
+
+    def get_n_brt_nodes(self) -> int:
+        return self.get_n_unique() - 1
+
+    def get_n_octree_nodes(self) -> int:
+        if self._c.n_octree_nodes == COUNT_UNSET:
+            raise RuntimeError("n_octree_nodes is not set")
+        return int(self._c.n_octree_nodes)
+
+    # -- host views -------------------------------------------------------------
+    def _keys_np(self, t) -> np.ndarray:
+        a = t.cpu().numpy()
+        return a.view(np.uint32 if self.key_bits == 32 else np.uint64)
+
+    def results(self) -> dict:
+        """Every output, copied to host and cut to its meaningful length."""
+        u = self.get_n_unique()
+        b = u - 1
+        m = self.get_n_octree_nodes()
+        return {
+            "sorted_keys": self._keys_np(self.u_morton_keys_alt),
+            "unique_keys": self._keys_np(self.u_morton_keys)[:u],
+            "n_unique": u,
+            "prefix_n": self.brt_prefix_n[:b].cpu().numpy(),
+            "has_leaf_left": self.brt_has_leaf_left[:b].cpu().numpy(),
+            "has_leaf_right": self.brt_has_leaf_right[:b].cpu().numpy(),
+            "left_child": self.brt_left_child[:b].cpu().numpy(),
+            "parents": self.brt_parents[:b].cpu().numpy(),
+            "edge_count": self.u_edge_count[:b].cpu().numpy(),
+            "edge_offset": self.u_edge_offset[:b].cpu().numpy(),
+            "n_octree_nodes": m,
+            "children": self.oct_children[:m].cpu().numpy(),
+            "corner": self.oct_corner[:m].cpu().numpy(),
+            "cell_size": self.oct_cell_size[:m].cpu().numpy(),
+            "child_node_mask": self.oct_child_node_mask[:m].cpu().numpy(),
+            "child_leaf_mask": self.oct_child_leaf_mask[:m].cpu().numpy(),
+        }
+
+
+def _stage(k: int):
+    fn_name = f"rw_tree_run_stage{k}"
+
+    def run(app: AppData, im: ImStorage, stream=None) -> None:
+        _check(getattr(lib(), fn_name)(ctypes.byref(app.c), im.handle,
+                                       _stream_handle(stream)), f"run_stage{k}")
+
+    run.__name__ = f"run_stage{k}"
+    run.__doc__ = f"cuda::run_stage{k} (cu_dispatcher.cuh:8-19); synchronous."
+    return run
+
+
+run_stage1, run_stage2, run_stage3, run_stage4, run_stage5, run_stage6, run_stage7 = (
+    _stage(k) for k in range(1, 8))
+
+
+def pipeline_enqueue(app: AppData, im: ImStorage, stream=None) -> None:
+    _check(lib().rw_tree_pipeline_enqueue(ctypes.byref(app.c), im.handle,
+                                          _stream_handle(stream)), "pipeline_enqueue")
+
+
+def pipeline_finish(app: AppData, im: ImStorage, stream=None) -> None:
+    _check(lib().rw_tree_pipeline_finish(ctypes.byref(app.c), im.handle,
+                                         _stream_handle(stream)), "pipeline_finish")
+
+
+def run_pipeline(app: AppData, im: ImStorage, stream=None) -> None:
+    """All seven stages, fused, one host synchronisation at the end."""
+    pipeline_enqueue(app, im, stream)
+    pipeline_finish(app, im, stream)
+
+
+def profile_pipeline(app: AppData, im: ImStorage, reps: int = 5, stream=None) -> dict:
+    """Mean device milliseconds of every kernel of the fused pipeline."""
+    ms = (ctypes.c_float * 64)()
+    nk = ctypes.c_int32()
+    _check(lib().rw_tree_pipeline_profile(ctypes.byref(app.c), im.handle,
+                                          _stream_handle(stream), reps, ms, 64,
+                                          ctypes.byref(nk)), "pipeline_profile")
+    names = lib().rw_tree_pipeline_kernel_names(im.handle).decode().split(",")
+    return {names[i]: float(ms[i]) for i in range(nk.value)}
+
+
+def run_host(app: AppData, im: ImStorage, h_points: np.ndarray,
+             out: Optional[dict] = None, stream=None) -> None:
+    """End to end from host memory; `out` maps rw_tree_host_out field names to
+    preallocated (ideally pinned) host arrays."""
+    pts = np.ascontiguousarray(h_points, np.float32)
+    ho = _HostOutC()
+    keep = []
+    for name, arr in (out or {}).items():
+        a = arr if isinstance(arr, np.ndarray) else arr.numpy()
+        keep.append(a)
+        setattr(ho, name, a.ctypes.data)
+    _check(lib().rw_tree_run_host(ctypes.byref(app.c), im.handle, pts.ctypes.data_as(_vp),
+                                  ctypes.byref(ho), _stream_handle(stream)), "run_host")

@@ -1,0 +1,149 @@
+// Device-side building blocks shared by the tree kernels (sm_100a only).
+//
+// Single-pass scans use decoupled look-back: every tile publishes a 32-bit
+// descriptor (bits 1:0 flag, bits 31:2 value) - first its own aggregate, then
+// its inclusive prefix once the predecessors' are known.  Every wait on a
+// predecessor is bounded; on timeout the tile records RW_ERR_TIMEOUT in the
+// device status word and publishes a (wrong but final) inclusive value so that
+// no successor waits on it, and the host reports the error.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rw_tree.h"
+
+namespace rwt {
+
+// Device-resident counts and error word, mirrored to pinned host memory.
+struct DevStatus {
+  uint32_t n_unique;        // written by the unique kernel's last tile
+  uint32_t n_octree_nodes;  // written by the scan's last tile
+  int32_t err;              // first rw_status error seen on the device
+  uint32_t err_site;        // which kernel reported it
+};
+
+enum : uint32_t { kFlagAgg = 1u, kFlagInc = 2u, kFlagMask = 3u };
+enum : uint32_t {
+  kSiteSort = 1,
+  kSiteUnique = 2,
+  kSiteScan = 3,
+  kSiteTree = 4,
+  kSiteOctree = 5
+};
+
+// ~1 s of polling with back-off before a wait gives up.
+constexpr uint32_t kSpinLimit = 1u << 21;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ void report_error(DevStatus* st, int32_t code,
+                                             uint32_t site) {
+  if (atomicCAS(reinterpret_cast<int*>(&st->err), 0, code) == 0)
+    st->err_site = site;
+}
+
+__device__ __forceinline__ bool device_failed(const DevStatus* st) {
+  return *reinterpret_cast<const volatile int32_t*>(&st->err) != 0;
+}
+
+__device__ __forceinline__ void backoff(uint32_t spin) {
+  if (spin > 64) __nanosleep(spin > 4096 ? 512 : 64);
+}
+
+// Inclusive warp scan (Kogge-Stone over shuffles).
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const T u = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= (uint32_t)d) v += u;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread.  `s_warp` needs
+// THREADS/32 entries.  Returns the exclusive prefix; *total gets the sum.
+template <int THREADS, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* total) {
+  constexpr int NW = THREADS / 32;
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const T inc = warp_inclusive_scan(v);
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < (uint32_t)NW ? s_warp[lane] : T(0);
+    const T wi = warp_inclusive_scan(w);
+    if (lane < (uint32_t)NW) s_warp[lane] = wi - w;
+    if (lane == NW - 1) s_warp[NW] = wi;
+  }
+  __syncthreads();
+  const T out = s_warp[warp] + inc - v;
+  *total = s_warp[NW];
+  __syncthreads();
+  return out;
+}
+
+// Warp-cooperative look-back for a single-value chained scan.  Called by one
+// whole warp of the tile `tile` (> 0).  desc[t] holds tile t's descriptor.
+// Returns the exclusive prefix of `tile` (sum of all earlier tiles).  On a
+// timeout it reports the error and returns 0.
+__device__ __forceinline__ uint32_t warp_lookback(const uint32_t* desc,
+                                                  uint32_t tile,
+                                                  DevStatus* st,
+                                                  uint32_t site) {
+  const uint32_t lane = lane_id();
+  uint32_t excl = 0;
+  int64_t hi = (int64_t)tile - 1;  // nearest predecessor still to read
+  uint32_t spin = 0;
+  while (true) {
+    const int64_t idx = hi - (int64_t)lane;
+    const uint32_t d = idx >= 0 ? ld_relaxed(desc + idx) : (kFlagInc);
+    const uint32_t f = d & kFlagMask;
+    const uint32_t inc_mask = __ballot_sync(0xffffffffu, f == kFlagInc);
+    const uint32_t bad_mask = __ballot_sync(0xffffffffu, f == 0u);
+    // lanes up to and including the first inclusive descriptor count
+    const uint32_t first_inc = inc_mask ? (uint32_t)(__ffs(inc_mask) - 1) : 32u;
+    const uint32_t need = first_inc == 32u ? 0xffffffffu
+                                           : (first_inc == 31u ? 0xffffffffu
+                                                               : ((2u << first_inc) - 1u));
+    if (bad_mask & need) {
+      if (++spin > kSpinLimit || device_failed(st)) {
+        if (lane == 0) report_error(st, RW_ERR_TIMEOUT, site);
+        return 0;
+      }
+      backoff(spin);
+      continue;
+    }
+    const uint32_t mine = ((need >> lane) & 1u) ? (d >> 2) : 0u;
+    excl += warp_sum(mine);
+    if (first_inc != 32u) return excl;
+    hi -= 32;
+  }
+}
+
+}  // namespace rwt

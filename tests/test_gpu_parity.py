@@ -1,0 +1,166 @@
+"""GPU parity: every output of the sm_100a pipeline equals the oracle's,
+bit for bit, through the C ABI (per-stage calls and the fused pipeline)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR
+from oracle import ORC_OK, compare  # noqa: F401
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("sorted_keys", "unique_keys", "prefix_n", "has_leaf_left", "has_leaf_right",
+          "left_child", "parents", "edge_count", "edge_offset", "children", "corner",
+          "cell_size", "child_node_mask", "child_leaf_mask")
+
+
+def run_gpu(rw, pts, key_bits=32, radix_bits=0, fused=True, app=None, im=None):
+    n = pts.shape[0]
+    if app is None:
+        app = rw.AppData(n, key_bits, points=pts)
+    else:
+        app.set_points(pts)
+    im = im or rw.ImStorage(n, key_bits, radix_bits)
+    if fused:
+        rw.run_pipeline(app, im)
+    else:
+        for k in range(1, 8):
+            getattr(rw, f"run_stage{k}")(app, im)
+    return app.results()
+
+
+def assert_same(got, want_res, label=""):
+    want = want_res.trimmed()
+    assert got["n_unique"] == want["n_unique"], label
+    assert got["n_octree_nodes"] == want["n_octree_nodes"], label
+    bad = [k for k in FIELDS
+           if np.ascontiguousarray(got[k]).tobytes() != np.ascontiguousarray(want[k]).tobytes()]
+    assert not bad, f"{label}: mismatching outputs {bad}"
+
+
+def cloud(rw, n, kind, seed):
+    if kind == "appdata":
+        return rw.generate_points(n, rw.GEN_APPDATA, seed)
+    if kind == "uniform":
+        return rw.generate_points(n, rw.GEN_UNIFORM, seed)
+    return rw.generate_points(n, rw.GEN_GAUSSIAN_MIXTURE, seed, n_components=8,
+                              sigma_lo=2.0, sigma_hi=20.0)
+
+
+def test_config1_stagewise_and_fused(rw, oracle):
+    pts = rw.generate_points(640 * 480, rw.GEN_APPDATA, 114514)
+    want = oracle.run(pts)
+    with open(os.path.join(GOLDEN_DIR, "config1_kat.json")) as f:
+        kat = json.load(f)
+    for fused in (False, True):
+        got = run_gpu(rw, pts, fused=fused)
+        assert_same(got, want, f"config1 fused={fused}")
+        assert got["n_unique"] == kat["n_unique"]
+        assert got["n_octree_nodes"] == kat["n_octree_nodes"]
+        for k in FIELDS:
+            assert f"{oracle.fnv1a64(np.ascontiguousarray(got[k])):#018x}" == kat["fnv1a64"][k], k
+
+
+def test_golden_small_cases(rw, oracle):
+    z = np.load(os.path.join(GOLDEN_DIR, "small_cases.npz"))
+    names = sorted({k.split("/")[0] for k in z.files})
+    for name in names:
+        pts = z[f"{name}/points"]
+        if int(z[f"{name}/status"][0]) != ORC_OK:
+            continue
+        for fused in (False, True):
+            got = run_gpu(rw, pts, fused=fused)
+            for k in FIELDS:
+                assert np.ascontiguousarray(got[k]).tobytes() == z[f"{name}/{k}"].tobytes(), \
+                    (name, fused, k)
+
+
+SIZES = (3, 31, 32, 33, 255, 256, 257, 1023, 1024, 1025, 4095, 4096, 4097,
+         6143, 6144, 6145, 8191, 8192, 8193, 65537)
+
+
+@pytest.mark.parametrize("key_bits,radix_bits", [(32, 8), (32, 11), (64, 8), (64, 11)])
+def test_ragged_sizes(rw, oracle, key_bits, radix_bits):
+    for i, n in enumerate(SIZES):
+        for kind in ("uniform", "gauss"):
+            pts = cloud(rw, n, kind, 1000 + i)
+            want = oracle.run(pts, key_bits=key_bits)
+            for fused in (False, True):
+                if want.status != ORC_OK:
+                    continue
+                got = run_gpu(rw, pts, key_bits, radix_bits, fused)
+                assert_same(got, want, f"n={n} {kind} k{key_bits} r{radix_bits} f{fused}")
+
+
+@pytest.mark.parametrize("key_bits", [32, 64])
+def test_one_million_both_forms(rw, oracle, key_bits):
+    for kind in ("uniform", "gauss"):
+        pts = cloud(rw, (1 << 20) + 1, kind, 77)
+        want = oracle.run(pts, key_bits=key_bits)
+        assert want.status == ORC_OK
+        for fused in (False, True):
+            assert_same(run_gpu(rw, pts, key_bits, 0, fused), want, f"{kind} fused={fused}")
+
+
+def test_buffers_reused_across_inputs(rw, oracle):
+    """A second cloud through the same AppData/ImStorage leaves no trace of the first."""
+    n = 50000
+    a, b = cloud(rw, n, "uniform", 1), cloud(rw, n, "gauss", 2)
+    app = rw.AppData(n, 32, points=a)
+    im = rw.ImStorage(n, 32)
+    rw.run_pipeline(app, im)
+    app.set_points(b)
+    rw.run_pipeline(app, im)
+    assert_same(app.results(), oracle.run(b), "reuse fused")
+    app.set_points(a)
+    for k in range(1, 8):
+        getattr(rw, f"run_stage{k}")(app, im)
+    assert_same(app.results(), oracle.run(a), "reuse stagewise")
+
+
+def test_sort_stage_matches_numpy(rw):
+    """Stage 2 alone on adversarial key sets."""
+    import torch
+    rng = np.random.default_rng(5)
+    for n, top in ((100000, 1 << 30), (100000, 2), (77777, 1), (8192 * 3 + 5, 1 << 8)):
+        keys = rng.integers(0, top, size=n, dtype=np.uint64).astype(np.uint32)
+        app = rw.AppData(n, 32, points=np.zeros((n, 4), np.float32))
+        app.u_morton_keys.copy_(torch.from_numpy(keys.view(np.int32)))
+        im = rw.ImStorage(n, 32)
+        rw.run_stage2(app, im)
+        got = app.u_morton_keys_alt.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, np.sort(keys)), (n, top)
+
+
+def test_degenerate_and_counts(rw):
+    n = 1000
+    pts = np.zeros((n, 4), np.float32)
+    app = rw.AppData(n, 32, points=pts)
+    im = rw.ImStorage(n, 32)
+    with pytest.raises(RuntimeError):
+        app.get_n_unique()  # unset, as app_data.hpp:110-116
+    for k in (1, 2, 3):
+        getattr(rw, f"run_stage{k}")(app, im)
+    assert app.get_n_unique() == 1
+    with pytest.raises(rw.RwTreeError) as e:
+        rw.run_stage4(app, im)
+    assert e.value.code == rw.RW_ERR_DEGENERATE
+    with pytest.raises(rw.RwTreeError) as e:
+        rw.run_pipeline(app, im)
+    assert e.value.code == rw.RW_ERR_DEGENERATE
+    # the device is still usable afterwards
+    good = cloud(rw, n, "uniform", 3)
+    app.set_points(good)
+    rw.run_pipeline(app, im)
+    assert app.get_n_unique() > 900
+
+
+def test_stage_order_enforced(rw):
+    n = 1000
+    app = rw.AppData(n, 32, points=cloud(rw, n, "uniform", 4))
+    im = rw.ImStorage(n, 32)
+    with pytest.raises(rw.RwTreeError) as e:
+        rw.run_stage4(app, im)
+    assert e.value.code == rw.RW_ERR_NOT_READY
