@@ -50,6 +50,10 @@ def parse_args():
     p.add_argument("--seed", type=int, default=20260101)
     p.add_argument("--no-verify", action="store_true", help="skip the oracle check")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sort-variant", type=int, default=-1,
+                   help="onesweep variant index (default: the storage's default)")
+    p.add_argument("--only-device", action="store_true",
+                   help="time only the device-resident pipeline (for profiler runs)")
     return p.parse_args()
 
 
@@ -261,6 +265,8 @@ def main():
     pts = make_points(rw, a.n, a.dist, a.seed + rank)
     app = rw.AppData(a.n, a.key_bits, points=pts)
     im = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
+    if a.sort_variant >= 0:
+        im.set_sort_variant(a.sort_variant)
     passes = -(-(30 if a.key_bits == 32 else 63) // (a.radix_bits or 8))
 
     def barrier():
@@ -303,6 +309,14 @@ def main():
     rw.pipeline_finish(app, im)
     ms_step = max_over_ranks(ev0.elapsed_time(ev1) / a.steps)
     value = a.n * world / (ms_step / 1e3)
+    if a.only_device:
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "points/s",
+                              "ms_per_step": ms_step, "only_device": True,
+                              "mismatches_vs_oracle": mismatches}), flush=True)
+        return 0
 
     # ---- per-kernel device times inside the pipeline -----------------------
     kms = rw.profile_pipeline(app, im, reps=max(3, min(10, a.steps)))

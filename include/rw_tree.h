@@ -100,6 +100,17 @@ int rw_tree_im_storage_create(uint32_t n_input, int32_t key_bits,
  * The reference fixes 8-bit digits (cu_dispatcher.cu:25-27). */
 int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
                                  int32_t radix_bits, rw_tree_im_storage** out);
+/* The onesweep sort comes in a menu of variants (threads per CTA, keys per
+ * thread, warp ranking scheme: 0 ballot multi-split, 1 match.any,
+ * 2 shared-memory atomic OR) for each key and digit width; the autotuner
+ * picks one per size class.  No reference counterpart (the reference fixes
+ * 512 threads x 15 keys with ballots, cu_dispatcher.cu:44-49). */
+int rw_tree_sort_variant_count(void);
+int rw_tree_sort_variant_info(int32_t idx, int32_t* key_bits, int32_t* radix_bits,
+                              int32_t* threads, int32_t* keys_per_thread,
+                              int32_t* rank_mode);
+/* Selects variant idx (its key and digit width must match the storage). */
+int rw_tree_im_storage_set_sort_variant(rw_tree_im_storage* im, int32_t idx);
 /* ~ImStorage (im_storage.cu:42-52). */
 int rw_tree_im_storage_destroy(rw_tree_im_storage* im);
 /* ImStorage::clearSmem (im_storage.cu:53-60): zeroes histograms, descriptors

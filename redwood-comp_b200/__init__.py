@@ -87,7 +87,8 @@ EXPORTS = (
     "rw_tree_run_stage6", "rw_tree_run_stage7", "rw_tree_pipeline_enqueue",
     "rw_tree_pipeline_finish", "rw_tree_run_host", "rw_tree_generate_points",
     "rw_tree_last_error", "rw_tree_version", "rw_tree_pipeline_profile",
-    "rw_tree_pipeline_kernel_names",
+    "rw_tree_pipeline_kernel_names", "rw_tree_sort_variant_count",
+    "rw_tree_sort_variant_info", "rw_tree_im_storage_set_sort_variant",
 )
 
 
@@ -115,6 +116,19 @@ def lib() -> ctypes.CDLL:
 def _check(rc: int, where: str) -> None:
     if rc != RW_OK:
         raise RwTreeError(rc, where, lib().rw_tree_last_error().decode())
+
+
+def sort_variants() -> list:
+    """The onesweep variant menu: dicts of key_bits, radix_bits, threads,
+    keys_per_thread, rank (0 ballot, 1 match.any, 2 smem atomic-or)."""
+    out = []
+    L = lib()
+    v = [ctypes.c_int32() for _ in range(5)]
+    for i in range(L.rw_tree_sort_variant_count()):
+        _check(L.rw_tree_sort_variant_info(i, *[ctypes.byref(x) for x in v]), "variant_info")
+        out.append(dict(index=i, key_bits=v[0].value, radix_bits=v[1].value,
+                        threads=v[2].value, keys_per_thread=v[3].value, rank=v[4].value))
+    return out
 
 
 def octree_capacity(n: int) -> int:
@@ -153,6 +167,10 @@ class ImStorage:
     @property
     def handle(self) -> _vp:
         return self._h
+
+    def set_sort_variant(self, idx: int) -> None:
+        _check(lib().rw_tree_im_storage_set_sort_variant(self._h, idx), "set_sort_variant")
+        self.sort_variant = idx
 
     def clear(self, stream=None) -> None:
         _check(lib().rw_tree_im_storage_clear(self._h, _stream_handle(stream)), "clearSmem")

@@ -14,10 +14,6 @@
 
 #include "internal.hpp"
 
-namespace rwt {
-uint32_t sort_tile_for(int key_bits, int radix_bits);
-}
-
 namespace {
 
 thread_local std::string g_last_error;
@@ -147,6 +143,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
   im->num_sms = sms;
   im->radix_bits = radix_bits == 0 ? 8 : radix_bits;
   im->passes = (code_bits(key_bits) + im->radix_bits - 1) / im->radix_bits;
+  im->sort_variant = rwt::default_sort_variant(key_bits, im->radix_bits);
   im->sort_tile = rwt::sort_tile_for(key_bits, im->radix_bits);
   im->sort_tiles = rwt::div_up(n_input, im->sort_tile);
   const size_t radix = size_t(1) << im->radix_bits;
@@ -183,6 +180,27 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
     return cuda_fail(e, "rw_tree_im_storage_create");
   }
   *out = im;
+  return RW_OK;
+}
+
+int rw_tree_sort_variant_count(void) { return rwt::sort_variant_count(); }
+
+int rw_tree_sort_variant_info(int32_t idx, int32_t* key_bits, int32_t* radix_bits,
+                              int32_t* threads, int32_t* keys_per_thread,
+                              int32_t* rank_mode) {
+  if (!key_bits || !radix_bits || !threads || !keys_per_thread || !rank_mode)
+    return RW_ERR_ARG;
+  return rwt::sort_variant_info(idx, key_bits, radix_bits, threads, keys_per_thread,
+                                rank_mode) == 0
+             ? RW_OK
+             : RW_ERR_ARG;
+}
+
+int rw_tree_im_storage_set_sort_variant(rw_tree_im_storage* im, int32_t idx) {
+  int kb, rb, th, kpt, rk;
+  if (!im || rwt::sort_variant_info(idx, &kb, &rb, &th, &kpt, &rk) != 0) return RW_ERR_ARG;
+  if (kb != im->key_bits || rb != im->radix_bits) return RW_ERR_ARG;
+  im->sort_variant = idx;
   return RW_OK;
 }
 

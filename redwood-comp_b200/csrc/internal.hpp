@@ -19,6 +19,7 @@ struct rw_tree_im_storage {
   // sort configuration (radix bits, passes, tile) fixed at creation
   int radix_bits = 8;
   int passes = 4;
+  int sort_variant = 0;      // index into the onesweep variant menu (k_keys.cu)
   uint32_t sort_tile = 0;
   uint32_t sort_tiles = 0;  // tiles per pass at n_cap
 
@@ -49,8 +50,8 @@ constexpr uint32_t kUniqueThreads = 256, kUniqueKpt = 16;
 constexpr uint32_t kUniqueTile = kUniqueThreads * kUniqueKpt;
 constexpr uint32_t kScanThreads = 256, kScanKpt = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanKpt;
-constexpr uint32_t kTreeThreads = 256;
-constexpr uint32_t kTreeTile = kTreeThreads;
+constexpr int kTreeThreads = 256, kTreeNpt = 4, kTreeHalo = 256;
+constexpr uint32_t kTreeTile = kTreeThreads * kTreeNpt;
 
 inline uint32_t div_up(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 
@@ -59,6 +60,13 @@ struct Count {
   const uint32_t* ptr;
   uint32_t value;
 };
+
+// ---- onesweep variant menu (k_keys.cu) --------------------------------------
+uint32_t sort_tile_for(int key_bits, int radix_bits);
+int sort_variant_count();
+int sort_variant_info(int idx, int* key_bits, int* radix_bits, int* threads, int* kpt,
+                      int* rank);
+int default_sort_variant(int key_bits, int radix_bits);
 
 // ---- launchers (each returns the launch's cudaError_t) --------------------
 

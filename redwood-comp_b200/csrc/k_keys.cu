@@ -131,10 +131,14 @@ __device__ __forceinline__ void digit_exclusive_scan(const uint32_t* s_cnt,
   }
 }
 
-// Stable rank of each key among equal digits inside a warp's 32-wide slice:
-// returns the mask of lanes holding the same digit (only valid lanes).
+// Warp ranking schemes: all return, for each lane, the mask of valid lanes in
+// its warp holding the same digit (the lane's stable rank is the popcount of
+// the mask below it).
+enum RankMode : int { kRankBallot = 0, kRankMatchAny = 1, kRankAtomicOr = 2 };
+
+// D ballots, one per digit bit (warp-level multi-split).
 template <int D>
-__device__ __forceinline__ uint32_t match_digit(uint32_t digit, uint32_t valid_mask) {
+__device__ __forceinline__ uint32_t match_ballot(uint32_t digit, uint32_t valid_mask) {
   uint32_t peers = valid_mask;
 #pragma unroll
   for (int b = 0; b < D; ++b) {
@@ -145,35 +149,44 @@ __device__ __forceinline__ uint32_t match_digit(uint32_t digit, uint32_t valid_m
   return peers;
 }
 
-template <typename K, int D, int THREADS, int KPT>
+template <typename K, int D, int THREADS, int KPT, int RANK>
 struct BinCfg {
   static constexpr int RADIX = 1 << D;
   static constexpr int NW = THREADS / 32;
   static constexpr int TILE = THREADS * KPT;
   static constexpr size_t kKeysBytes = size_t(TILE) * sizeof(K);
   static constexpr size_t kHistBytes = size_t(NW) * RADIX * 4;
+  static constexpr size_t kMatchBytes = RANK == kRankAtomicOr ? kHistBytes : 0;
   static constexpr size_t kSmem =
-      kKeysBytes + kHistBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
+      kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
 };
 
-template <typename K, int D, int THREADS, int KPT>
-__global__ void __launch_bounds__(THREADS)
+// One onesweep pass over `n` keys: digit `shift`..`shift+D-1`, stable.
+// desc: [(tiles + 1) x RADIX] descriptors, row 0 prefilled with the global
+// exclusive digit offsets (k_sort_init), rows 1.. zero.
+template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, uint32_t n,
               int shift, uint32_t* __restrict__ desc,
               uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
-  using C = BinCfg<K, D, THREADS, KPT>;
+  using C = BinCfg<K, D, THREADS, KPT, RANK>;
   constexpr int RADIX = C::RADIX, NW = C::NW, TILE = C::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
   K* s_keys = reinterpret_cast<K*>(smem);
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem + C::kKeysBytes);
-  uint32_t* s_cnt = s_hist + NW * RADIX;
+  uint32_t* s_match = s_hist + NW * RADIX;  // only with kRankAtomicOr
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + C::kKeysBytes + C::kHistBytes +
+                                                C::kMatchBytes);
   uint32_t* s_start = s_cnt + RADIX;
   uint32_t* s_gofs = s_start + RADIX;
   uint32_t* s_misc = s_gofs + RADIX;  // [0] tile, [1..] warp scan scratch
 
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   if (tid == 0) s_misc[0] = atomicAdd(tile_ctr, 1u);
-  for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] = 0;
+  for (int i = tid; i < NW * RADIX; i += THREADS) {
+    s_hist[i] = 0;
+    if (RANK == kRankAtomicOr) s_match[i] = 0;
+  }
   __syncthreads();
   const uint32_t tile = s_misc[0];
   const uint32_t base = tile * TILE;
@@ -190,18 +203,30 @@ __global__ void __launch_bounds__(THREADS)
 
   // per-warp stable ranks (key order inside the warp = step, then lane)
   uint32_t* wh = s_hist + warp * RADIX;
+  uint32_t* wm = s_match + warp * RADIX;
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
     const uint32_t idx = wbase + 32u * i;
     const bool valid = idx < n;
     const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-    const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-    const uint32_t peers = match_digit<D>(dig, vmask);
+    uint32_t peers;
+    if (RANK == kRankBallot) {
+      peers = match_ballot<D>(dig, __ballot_sync(0xffffffffu, valid));
+    } else if (RANK == kRankMatchAny) {
+      peers = __match_any_sync(0xffffffffu, valid ? dig : 0xffffffffu);
+      if (!valid) peers = 0;
+    } else {
+      if (valid) atomicOr(&wm[dig], 1u << lane);
+      __syncwarp();
+      peers = valid ? wm[dig] : 0u;
+    }
     const uint32_t below = __popc(peers & lanemask_lt());
     uint32_t prev = 0;
+    if (RANK == kRankAtomicOr) __syncwarp();
     if (valid && below == 0) {
       prev = wh[dig];
       wh[dig] = prev + __popc(peers);
+      if (RANK == kRankAtomicOr) wm[dig] = 0;
     }
     const int leader = valid ? __ffs(peers) - 1 : int(lane);
     prev = __shfl_sync(0xffffffffu, prev, leader);
@@ -210,7 +235,8 @@ __global__ void __launch_bounds__(THREADS)
   }
   __syncthreads();
 
-  // per digit: exclusive scan over warps, publish the tile aggregate
+  // per digit: exclusive scan over warps, publish the tile aggregate, then
+  // look back at once so the inclusive prefix is out as early as possible
   uint32_t* drow = desc + size_t(tile + 1) * RADIX;
   for (int d = tid; d < RADIX; d += THREADS) {
     uint32_t run = 0;
@@ -223,21 +249,6 @@ __global__ void __launch_bounds__(THREADS)
     s_cnt[d] = run;
     st_relaxed(drow + d, kFlagAgg | (run << 2));
   }
-  __syncthreads();
-  digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
-  __syncthreads();
-
-  // reorder the tile by digit in shared memory
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    const uint32_t idx = wbase + 32u * i;
-    if (idx < n) {
-      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-      s_keys[s_start[dig] + wh[dig] + rank[i]] = keys[i];
-    }
-  }
-
-  // per digit: decoupled look-back over the previous tiles
   for (int d = tid; d < RADIX; d += THREADS) {
     uint32_t excl = 0;
     int64_t k = tile;  // row k holds tile k-1's descriptor (row 0: global)
@@ -262,8 +273,22 @@ __global__ void __launch_bounds__(THREADS)
       backoff(spin);
     }
     st_relaxed(drow + d, kFlagInc | ((excl + s_cnt[d]) << 2));
-    s_gofs[d] = excl - s_start[d];
+    s_gofs[d] = excl;
   }
+  __syncthreads();
+  digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
+  __syncthreads();
+
+  // reorder the tile by digit in shared memory
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t idx = wbase + 32u * i;
+    if (idx < n) {
+      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
+      s_keys[s_start[dig] + wh[dig] + rank[i]] = keys[i];
+    }
+  }
+  for (int d = tid; d < RADIX; d += THREADS) s_gofs[d] -= s_start[d];
   __syncthreads();
 
   // write runs of equal digits to their global positions
@@ -317,32 +342,28 @@ cudaError_t histogram_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
   return cudaGetLastError();
 }
 
-template <typename K, int D, int THREADS, int KPT>
+template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 cudaError_t passes_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
                      cudaStream_t s, cudaEvent_t* marks) {
-  using C = BinCfg<K, D, THREADS, KPT>;
+  using C = BinCfg<K, D, THREADS, KPT, RANK>;
+  auto kern = k_binning<K, D, THREADS, KPT, RANK, MINB>;
   const uint32_t n = app.n_input;
   const uint32_t tiles = div_up(n, C::TILE);
   const uint32_t rows = im->sort_tiles + 1;
+  if (tiles > im->sort_tiles) return cudaErrorInvalidValue;
   k_sort_init<D><<<im->passes, 256, 0, s>>>(im->d_ghist, im->d_sort_desc, rows);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
-  static bool attr_set = false;
-  if (!attr_set) {
-    e = cudaFuncSetAttribute(k_binning<K, D, THREADS, KPT>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(C::kSmem));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
+  if (e != cudaSuccess) return e;
   K* keys = static_cast<K*>(app.u_morton_keys);
   K* alt = static_cast<K*>(app.u_morton_keys_alt);
   K* tmp = static_cast<K*>(im->d_tmp_keys);
   const K* src = keys;
   for (int p = 0; p < im->passes; ++p) {
     K* dst = ((im->passes - 1 - p) % 2 == 0) ? alt : tmp;
-    k_binning<K, D, THREADS, KPT><<<tiles, THREADS, C::kSmem, s>>>(
+    kern<<<tiles, THREADS, C::kSmem, s>>>(
         src, dst, n, p * D, im->d_sort_desc + size_t(p) * rows * C::RADIX,
         im->d_tile_ctr + kCtrSortBase + p, im->d_status);
     e = cudaGetLastError();
@@ -353,12 +374,71 @@ cudaError_t passes_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
   return cudaSuccess;
 }
 
+using PassFn = cudaError_t (*)(const rw_tree_app_data&, rw_tree_im_storage*, cudaStream_t,
+                               cudaEvent_t*);
+
+struct SortVariant {
+  int key_bits, radix_bits, threads, kpt, rank;
+  PassFn fn;
+};
+
+// The menu the autotuner chooses from (entry 0 of each key/digit width is
+// the default).
+const SortVariant kVariants[] = {
+    {32, 8, 512, 16, kRankBallot, passes_t<uint32_t, 8, 512, 16, kRankBallot, 1>},
+    {32, 8, 512, 16, kRankMatchAny, passes_t<uint32_t, 8, 512, 16, kRankMatchAny, 1>},
+    {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 1>},
+    {32, 8, 256, 16, kRankBallot, passes_t<uint32_t, 8, 256, 16, kRankBallot, 2>},
+    {32, 8, 256, 16, kRankMatchAny, passes_t<uint32_t, 8, 256, 16, kRankMatchAny, 2>},
+    {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 2>},
+    {32, 8, 256, 32, kRankMatchAny, passes_t<uint32_t, 8, 256, 32, kRankMatchAny, 1>},
+    {32, 8, 256, 32, kRankAtomicOr, passes_t<uint32_t, 8, 256, 32, kRankAtomicOr, 1>},
+    {32, 8, 384, 16, kRankAtomicOr, passes_t<uint32_t, 8, 384, 16, kRankAtomicOr, 2>},
+    {32, 11, 256, 24, kRankBallot, passes_t<uint32_t, 11, 256, 24, kRankBallot, 1>},
+    {32, 11, 256, 24, kRankMatchAny, passes_t<uint32_t, 11, 256, 24, kRankMatchAny, 1>},
+    {32, 11, 256, 24, kRankAtomicOr, passes_t<uint32_t, 11, 256, 24, kRankAtomicOr, 1>},
+    {32, 11, 256, 16, kRankMatchAny, passes_t<uint32_t, 11, 256, 16, kRankMatchAny, 1>},
+    {32, 11, 512, 16, kRankMatchAny, passes_t<uint32_t, 11, 512, 16, kRankMatchAny, 1>},
+    {64, 8, 256, 16, kRankBallot, passes_t<uint64_t, 8, 256, 16, kRankBallot, 2>},
+    {64, 8, 256, 16, kRankMatchAny, passes_t<uint64_t, 8, 256, 16, kRankMatchAny, 2>},
+    {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},
+    {64, 8, 512, 16, kRankMatchAny, passes_t<uint64_t, 8, 512, 16, kRankMatchAny, 1>},
+    {64, 11, 256, 16, kRankBallot, passes_t<uint64_t, 11, 256, 16, kRankBallot, 1>},
+    {64, 11, 256, 16, kRankMatchAny, passes_t<uint64_t, 11, 256, 16, kRankMatchAny, 1>},
+    {64, 11, 256, 16, kRankAtomicOr, passes_t<uint64_t, 11, 256, 16, kRankAtomicOr, 1>},
+    {64, 11, 256, 8, kRankMatchAny, passes_t<uint64_t, 11, 256, 8, kRankMatchAny, 2>},
+};
+constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+
 }  // namespace
 
-// Sort tile per configuration; must match passes_t's instantiation below.
+// Smallest tile of any variant for this key/digit width: sizes the descriptors.
 uint32_t sort_tile_for(int key_bits, int radix_bits) {
-  if (key_bits == 32) return radix_bits == 8 ? 512 * 16 : 256 * 24;
-  return radix_bits == 8 ? 256 * 16 : 256 * 16;
+  uint32_t t = 0xffffffffu;
+  for (const auto& v : kVariants)
+    if (v.key_bits == key_bits && v.radix_bits == radix_bits)
+      t = std::min<uint32_t>(t, uint32_t(v.threads * v.kpt));
+  return t;
+}
+
+int sort_variant_count() { return kNumVariants; }
+
+int sort_variant_info(int idx, int* key_bits, int* radix_bits, int* threads, int* kpt,
+                      int* rank) {
+  if (idx < 0 || idx >= kNumVariants) return -1;
+  const auto& v = kVariants[idx];
+  *key_bits = v.key_bits;
+  *radix_bits = v.radix_bits;
+  *threads = v.threads;
+  *kpt = v.kpt;
+  *rank = v.rank;
+  return 0;
+}
+
+int default_sort_variant(int key_bits, int radix_bits) {
+  for (int i = 0; i < kNumVariants; ++i)
+    if (kVariants[i].key_bits == key_bits && kVariants[i].radix_bits == radix_bits) return i;
+  return -1;
 }
 
 cudaError_t launch_morton(const rw_tree_app_data& app, rw_tree_im_storage* im,
@@ -382,11 +462,11 @@ cudaError_t launch_histogram(const rw_tree_app_data& app, rw_tree_im_storage* im
 cudaError_t launch_sort_passes(const rw_tree_app_data& app,
                                rw_tree_im_storage* im, cudaStream_t s,
                                cudaEvent_t* marks) {
-  if (app.key_bits == 32)
-    return im->radix_bits == 8 ? passes_t<uint32_t, 8, 512, 16>(app, im, s, marks)
-                               : passes_t<uint32_t, 11, 256, 24>(app, im, s, marks);
-  return im->radix_bits == 8 ? passes_t<uint64_t, 8, 256, 16>(app, im, s, marks)
-                             : passes_t<uint64_t, 11, 256, 16>(app, im, s, marks);
+  const int v = im->sort_variant;
+  if (v < 0 || v >= kNumVariants || kVariants[v].key_bits != app.key_bits ||
+      kVariants[v].radix_bits != im->radix_bits)
+    return cudaErrorInvalidValue;
+  return kVariants[v].fn(app, im, s, marks);
 }
 
 }  // namespace rwt

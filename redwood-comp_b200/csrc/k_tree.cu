@@ -122,34 +122,48 @@ struct BrtNode {
   int d, j, gamma, dnode;
 };
 
-// n = n_brt_nodes; keys live in [0, n].
+// Key reads of the radix-tree search go through a shared-memory window of the
+// tile's keys plus a halo on either side; probes outside it read global memory.
 template <typename K>
-__device__ __forceinline__ BrtNode brt_node(int i, int n, const K* __restrict__ codes) {
-  const K ci = codes[i];
+struct KeyWindow {
+  const K* __restrict__ codes;
+  const K* win;  // shared memory
+  int lo;        // global index of win[0]
+  int len;
+  __device__ __forceinline__ K operator()(int j) const {
+    const int r = j - lo;
+    return uint32_t(r) < uint32_t(len) ? win[r] : codes[j];
+  }
+};
+
+// n = n_brt_nodes; keys live in [0, n].
+template <typename K, typename KeyAt>
+__device__ __forceinline__ BrtNode brt_node(int i, int n, const KeyAt& key) {
+  const K ci = key(i);
   int d;
   if (i == 0) {
     d = 1;
   } else {
-    const int diff = delta(ci, codes[i + 1]) - delta(ci, codes[i - 1]);
+    const int diff = delta(ci, key(i + 1)) - delta(ci, key(i - 1));
     d = (diff > 0) - (diff < 0);
   }
   int l = 0;
   if (i == 0) {
     l = n - 1;
   } else {
-    const int dmin = delta(ci, codes[i - d]);
+    const int dmin = delta(ci, key(i - d));
     int lmax = 2;
     while ((long long)i + (long long)lmax * d >= 0 && i + lmax * d <= n &&
-           delta(ci, codes[i + lmax * d]) > dmin)
+           delta(ci, key(i + lmax * d)) > dmin)
       lmax *= 2;
     const int lcut = (d == -1) ? i : n - i;
     for (int t = lmax / 2, div = 2; t >= 1; div *= 2, t = lmax / div)
-      if (l + t <= lcut && delta(ci, codes[i + (l + t) * d]) > dmin) l += t;
+      if (l + t <= lcut && delta(ci, key(i + (l + t) * d)) > dmin) l += t;
   }
   BrtNode r;
   r.d = d;
   r.j = i + l * d;
-  r.dnode = delta(ci, codes[r.j]);
+  r.dnode = delta(ci, key(r.j));
   int s = 0;
   const int maxdiv = 1 << log2_ceil_u(uint32_t(l));
   const int scut = (d == -1) ? i - 1 : n - i - 1;
@@ -157,7 +171,7 @@ __device__ __forceinline__ BrtNode brt_node(int i, int n, const K* __restrict__ 
   for (uint32_t t = (uint32_t(l) + 1u) / 2u; div <= maxdiv;
        div <<= 1, t = (uint32_t(l) + uint32_t(div) - 1u) / uint32_t(div)) {
     if (uint32_t(s) + t <= uint32_t(scut) &&
-        delta(ci, codes[uint32_t(i) + (uint32_t(s) + t) * uint32_t(d)]) > r.dnode)
+        delta(ci, key(int(uint32_t(i) + (uint32_t(s) + t) * uint32_t(d)))) > r.dnode)
       s += int(t);
   }
   r.gamma = i + s * d + min(d, 0);
@@ -169,8 +183,8 @@ __device__ __forceinline__ BrtNode brt_node(int i, int n, const K* __restrict__ 
 // true root of [0, n] (the reference's root covers only [0, n-1]; sequential
 // execution on a zeroed buffer leaves exactly those entries 0, and no other
 // node names them).  Every other entry is written once, by its true parent.
-template <typename K>
-__device__ __forceinline__ void write_node(int i, int n, const K* __restrict__ codes,
+template <typename K, typename KeyAt>
+__device__ __forceinline__ void write_node(int i, int n, const KeyAt& key,
                                            const BrtNode& r, uint8_t* prefix_n,
                                            uint8_t* hl, uint8_t* hr, int32_t* lc,
                                            int32_t* parents) {
@@ -185,26 +199,26 @@ __device__ __forceinline__ void write_node(int i, int n, const K* __restrict__ c
     if (!leaf_r) parents[r.gamma + 1] = i;
   } else {
     parents[0] = 0;
-    const int gamma_true =
-        delta(codes[n - 1], codes[n]) < r.dnode ? n - 1 : r.gamma;
+    const int gamma_true = delta(key(n - 1), key(n)) < r.dnode ? n - 1 : r.gamma;
     if (gamma_true > 0) parents[gamma_true] = 0;
     if (gamma_true + 1 < n) parents[gamma_true + 1] = 0;
   }
 }
 
 // Edge count of node i >= 1 without reading parent[] (see file comment).
-template <typename K>
-__device__ __forceinline__ int fused_edge_count(int i, int n, const K* __restrict__ codes,
+template <typename K, typename KeyAt>
+__device__ __forceinline__ int fused_edge_count(int i, int n, const KeyAt& key,
                                                 const BrtNode& r, int root_true_delta,
                                                 int root_prefix) {
   const int lo = min(i, r.j), hi = max(i, r.j);
-  const int dl = lo > 0 ? delta(codes[lo - 1], codes[lo]) : -1;
-  const int dr = hi < n ? delta(codes[hi], codes[hi + 1]) : -1;
+  const int dl = lo > 0 ? delta(key(lo - 1), key(lo)) : -1;
+  const int dr = hi < n ? delta(key(hi), key(hi + 1)) : -1;
   const int pd = max(dl, dr);
   const int parent_prefix = pd == root_true_delta ? root_prefix : pd;
   return r.dnode / 3 - parent_prefix / 3;
 }
 
+// Tile: kTreeThreads threads x kTreeNpt consecutive nodes each.
 template <typename K, bool FUSED>
 __global__ void __launch_bounds__(kTreeThreads)
     k_radix_tree(const K* __restrict__ codes, Count n_unique_c,
@@ -213,7 +227,9 @@ __global__ void __launch_bounds__(kTreeThreads)
                  int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
                  int32_t* __restrict__ edge_offset, uint32_t* __restrict__ desc,
                  uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
-  constexpr int NW = kTreeThreads / 32;
+  constexpr int NW = kTreeThreads / 32, NPT = kTreeNpt, HALO = kTreeHalo;
+  constexpr int WIN = kTreeTile + 2 * HALO;
+  __shared__ K s_win[WIN];
   __shared__ uint32_t s_warp[NW + 1];
   __shared__ uint32_t s_tile, s_excl;
   const uint32_t nu = count_of(n_unique_c);
@@ -238,16 +254,32 @@ __global__ void __launch_bounds__(kTreeThreads)
       ++iter;
     }
     if (tile >= n_tiles) break;
-    const int i = int(tile * kTreeTile + tid);
-    int ec = 0;
-    if (i < n) {
-      const BrtNode r = brt_node(i, n, codes);
-      write_node(i, n, codes, r, prefix_n, hl, hr, lc, parents);
-      if (FUSED && i > 0) ec = fused_edge_count(i, n, codes, r, root_true_delta, root_prefix);
+    const int base = int(tile) * kTreeTile;
+    const int wlo = base - HALO;
+    for (int j = tid; j < WIN; j += kTreeThreads) {
+      const int g = wlo + j;
+      s_win[j] = (g >= 0 && g <= n) ? codes[g] : K(0);
+    }
+    __syncthreads();
+    const KeyWindow<K> key{codes, s_win, wlo, WIN};
+    const int first = base + int(tid) * NPT;
+    int ec[NPT];
+    uint32_t local = 0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+      const int i = first + q;
+      ec[q] = 0;
+      if (i < n) {
+        const BrtNode r = brt_node<K>(i, n, key);
+        write_node<K>(i, n, key, r, prefix_n, hl, hr, lc, parents);
+        if (FUSED && i > 0)
+          ec[q] = fused_edge_count<K>(i, n, key, r, root_true_delta, root_prefix);
+      }
+      local += uint32_t(ec[q]);
     }
     if (FUSED) {
       uint32_t total;
-      const uint32_t ex = block_exclusive_scan<kTreeThreads>(uint32_t(ec), s_warp, &total);
+      const uint32_t ex = block_exclusive_scan<kTreeThreads>(local, s_warp, &total);
       if (warp == 0) {
         uint32_t excl = 0;
         if (tile == 0) {
@@ -263,12 +295,18 @@ __global__ void __launch_bounds__(kTreeThreads)
         }
       }
       __syncthreads();
-      if (i < n) {
-        edge_count[i] = ec;
-        edge_offset[i] = int32_t(s_excl + ex);
+      uint32_t run = s_excl + ex;
+#pragma unroll
+      for (int q = 0; q < NPT; ++q) {
+        const int i = first + q;
+        if (i < n) {
+          edge_count[i] = ec[q];
+          edge_offset[i] = int32_t(run);
+        }
+        run += uint32_t(ec[q]);
       }
-      __syncthreads();
     }
+    __syncthreads();  // the window is reloaded by the next tile
   }
 }
 

@@ -164,3 +164,30 @@ def test_stage_order_enforced(rw):
     with pytest.raises(rw.RwTreeError) as e:
         rw.run_stage4(app, im)
     assert e.value.code == rw.RW_ERR_NOT_READY
+
+
+def test_every_sort_variant_is_exact(rw, oracle):
+    """Each onesweep variant of the autotuner's menu sorts exactly and keeps
+    the whole pipeline bit-exact."""
+    import torch
+    rng = np.random.default_rng(11)
+    for v in rw.sort_variants():
+        kb, rb = v["key_bits"], v["radix_bits"]
+        kt = np.uint32 if kb == 32 else np.uint64
+        top = (1 << 30) if kb == 32 else (1 << 63)
+        for n in (1, 4097, 100003):
+            keys = rng.integers(0, top, size=n, dtype=np.uint64).astype(kt)
+            keys[: n // 3] = keys[0]  # a long run of one key
+            app = rw.AppData(n, kb, points=np.zeros((n, 4), np.float32))
+            app.u_morton_keys.copy_(torch.from_numpy(keys.view(np.int32 if kb == 32 else np.int64)))
+            im = rw.ImStorage(n, kb, rb)
+            im.set_sort_variant(v["index"])
+            rw.run_stage2(app, im)
+            got = app.u_morton_keys_alt.cpu().numpy().view(kt)
+            assert np.array_equal(got, np.sort(keys)), (v, n)
+        pts = cloud(rw, 30001, "gauss", 5)
+        app = rw.AppData(30001, kb, points=pts)
+        im = rw.ImStorage(30001, kb, rb)
+        im.set_sort_variant(v["index"])
+        rw.run_pipeline(app, im)
+        assert_same(app.results(), oracle.run(pts, key_bits=kb), f"variant {v}")
