@@ -148,9 +148,11 @@ def kernel_bytes(name, n, u, m, K):
         return 2 * K * n
     if name == "unique":
         return K * n + K * u
-    if name == "radix_tree_edges_scan":
-        # codes read; prefix_n, 2 leaf flags, left_child, parent, edge count, offset written
-        return K * u + 19 * b
+    if name == "radix_tree_edges":
+        # codes read; prefix_n, 2 leaf flags, left_child, parent, edge count written
+        return K * u + 15 * b
+    if name == "edge_scan":
+        return 8 * b
     if name == "octree_rows":
         # codes, prefix_n, count, offset read; corner 16 + cell 4 + children 32 + masks 8 written
         return (K + 9) * b + 60 * m
@@ -395,7 +397,7 @@ def main():
         "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
                               "frac": round(pipe_gbs / hbm, 4)},
         "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
-        "clocks": clocks.summary(), "gpu_launches": (6 + passes) * a.steps,
+        "clocks": clocks.summary(), "gpu_launches": (7 + passes) * a.steps,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -329,6 +329,8 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
   const rwt::Count nm{&im->d_status->n_octree_nodes, 0};
   RW_CUDA(rwt::launch_radix_tree(*app, im, nu, true, s));
   RW_CUDA(mark());
+  RW_CUDA(rwt::launch_edge_scan(*app, im, nu, s));
+  RW_CUDA(mark());
   RW_CUDA(rwt::launch_octree(*app, im, nu, nm, s, ev ? ev + k : nullptr));
   if (ev) k += 2;
   RW_CUDA(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(rwt::DevStatus),
@@ -348,7 +350,7 @@ const char* rw_tree_pipeline_kernel_names(const rw_tree_im_storage* im) {
   static thread_local std::string names;
   names = "morton_histogram,sort_init";
   for (int p = 0; p < (im ? im->passes : 0); ++p) names += ",sort_pass" + std::to_string(p);
-  names += ",unique,radix_tree_edges_scan,octree_rows,octree_links";
+  names += ",unique,radix_tree_edges,edge_scan,octree_rows,octree_links";
   return names.c_str();
 }
 
@@ -357,7 +359,7 @@ int rw_tree_pipeline_profile(rw_tree_app_data* app, rw_tree_im_storage* im,
                              int32_t max_kernels, int32_t* n_kernels) {
   if (!app || !im || !kernel_ms || reps < 1) return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int n_k = 6 + im->passes;
+  const int n_k = 7 + im->passes;
   if (max_kernels < n_k) return RW_ERR_ARG;
   cudaEvent_t ev[64];
   for (int i = 0; i <= n_k; ++i) RW_CUDA(cudaEventCreate(&ev[i]));

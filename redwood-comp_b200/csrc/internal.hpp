@@ -81,10 +81,10 @@ cudaError_t launch_sort_passes(const rw_tree_app_data& app,
                                cudaEvent_t* marks = nullptr);
 cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
                           cudaStream_t s);
-// Stage 4 alone (fused = false) or stages 4-6 in one pass (fused = true).
+// Stage 4 alone (edges = false) or stages 4 and 5 in one pass (edges = true).
 cudaError_t launch_radix_tree(const rw_tree_app_data& app,
                               rw_tree_im_storage* im, Count n_unique,
-                              bool fused, cudaStream_t s);
+                              bool edges, cudaStream_t s);
 cudaError_t launch_edge_count(const rw_tree_app_data& app,
                               rw_tree_im_storage* im, Count n_unique,
                               cudaStream_t s);

@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(256)
     k_sort_init(const uint32_t* __restrict__ ghist, uint32_t* __restrict__ desc,
                 uint32_t tiles_plus_one) {
   constexpr int RADIX = 1 << D;
-  constexpr int R = RADIX > 256 ? RADIX / 256 : 1;
+  constexpr int R = (RADIX + 255) / 256;
+  static_assert(R * 256 >= RADIX, "every digit needs an offset");
   __shared__ uint32_t s_warp[9];
   const int pass = blockIdx.x;
   const uint32_t* h = ghist + pass * RADIX;
@@ -115,7 +116,8 @@ __device__ __forceinline__ void digit_exclusive_scan(const uint32_t* s_cnt,
                                                      uint32_t* s_start,
                                                      uint32_t* s_warp) {
   constexpr int RADIX = 1 << D;
-  constexpr int R = RADIX > THREADS ? RADIX / THREADS : 1;
+  constexpr int R = (RADIX + THREADS - 1) / THREADS;  // digits per thread
+  static_assert(R * THREADS >= RADIX, "every digit needs a start offset");
   const int first = threadIdx.x * R;
   uint32_t local = 0;
 #pragma unroll
@@ -159,6 +161,7 @@ struct BinCfg {
   static constexpr size_t kMatchBytes = RANK == kRankAtomicOr ? kHistBytes : 0;
   static constexpr size_t kSmem =
       kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
+  static_assert(kSmem <= 227 * 1024, "onesweep variant exceeds shared memory per CTA");
 };
 
 // One onesweep pass over `n` keys: digit `shift`..`shift+D-1`, stable.
@@ -250,19 +253,32 @@ __global__ void __launch_bounds__(THREADS, MINB)
     st_relaxed(drow + d, kFlagAgg | (run << 2));
   }
   for (int d = tid; d < RADIX; d += THREADS) {
+    // walk back 4 descriptors per round trip; row 0 is always inclusive
     uint32_t excl = 0;
     int64_t k = tile;  // row k holds tile k-1's descriptor (row 0: global)
     uint32_t spin = 0;
     while (true) {
-      const uint32_t v = ld_relaxed(desc + size_t(k) * RADIX + d);
-      const uint32_t f = v & kFlagMask;
-      if (f == kFlagInc) {
-        excl += v >> 2;
-        break;
+      uint32_t v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        v[q] = k - q >= 0 ? ld_relaxed(desc + size_t(k - q) * RADIX + d) : kFlagInc;
+      bool done = false;
+      int used = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (done || used != q) break;
+        const uint32_t f = v[q] & kFlagMask;
+        if (f == kFlagInc) {
+          excl += v[q] >> 2;
+          done = true;
+        } else if (f == kFlagAgg) {
+          excl += v[q] >> 2;
+          ++used;
+        }
       }
-      if (f == kFlagAgg) {
-        excl += v >> 2;
-        --k;
+      if (done) break;
+      k -= used;
+      if (used) {
         spin = 0;
         continue;
       }
@@ -385,28 +401,27 @@ struct SortVariant {
 // The menu the autotuner chooses from (entry 0 of each key/digit width is
 // the default).
 const SortVariant kVariants[] = {
-    {32, 8, 512, 16, kRankBallot, passes_t<uint32_t, 8, 512, 16, kRankBallot, 1>},
-    {32, 8, 512, 16, kRankMatchAny, passes_t<uint32_t, 8, 512, 16, kRankMatchAny, 1>},
-    {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 1>},
-    {32, 8, 256, 16, kRankBallot, passes_t<uint32_t, 8, 256, 16, kRankBallot, 2>},
-    {32, 8, 256, 16, kRankMatchAny, passes_t<uint32_t, 8, 256, 16, kRankMatchAny, 2>},
-    {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 2>},
-    {32, 8, 256, 32, kRankMatchAny, passes_t<uint32_t, 8, 256, 32, kRankMatchAny, 1>},
-    {32, 8, 256, 32, kRankAtomicOr, passes_t<uint32_t, 8, 256, 32, kRankAtomicOr, 1>},
+    {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 2>},
     {32, 8, 384, 16, kRankAtomicOr, passes_t<uint32_t, 8, 384, 16, kRankAtomicOr, 2>},
-    {32, 11, 256, 24, kRankBallot, passes_t<uint32_t, 11, 256, 24, kRankBallot, 1>},
-    {32, 11, 256, 24, kRankMatchAny, passes_t<uint32_t, 11, 256, 24, kRankMatchAny, 1>},
+    {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 3>},
+    {32, 8, 256, 24, kRankAtomicOr, passes_t<uint32_t, 8, 256, 24, kRankAtomicOr, 2>},
+    {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 2>},
+    {32, 8, 512, 24, kRankAtomicOr, passes_t<uint32_t, 8, 512, 24, kRankAtomicOr, 1>},
+    {32, 8, 256, 16, kRankBallot, passes_t<uint32_t, 8, 256, 16, kRankBallot, 3>},
+    {32, 8, 512, 16, kRankBallot, passes_t<uint32_t, 8, 512, 16, kRankBallot, 1>},
+    {32, 8, 384, 16, kRankMatchAny, passes_t<uint32_t, 8, 384, 16, kRankMatchAny, 2>},
+    {32, 11, 512, 16, kRankBallot, passes_t<uint32_t, 11, 512, 16, kRankBallot, 1>},
+    {32, 11, 256, 16, kRankAtomicOr, passes_t<uint32_t, 11, 256, 16, kRankAtomicOr, 1>},
     {32, 11, 256, 24, kRankAtomicOr, passes_t<uint32_t, 11, 256, 24, kRankAtomicOr, 1>},
-    {32, 11, 256, 16, kRankMatchAny, passes_t<uint32_t, 11, 256, 16, kRankMatchAny, 1>},
-    {32, 11, 512, 16, kRankMatchAny, passes_t<uint32_t, 11, 512, 16, kRankMatchAny, 1>},
-    {64, 8, 256, 16, kRankBallot, passes_t<uint64_t, 8, 256, 16, kRankBallot, 2>},
-    {64, 8, 256, 16, kRankMatchAny, passes_t<uint64_t, 8, 256, 16, kRankMatchAny, 2>},
+    {32, 11, 256, 24, kRankBallot, passes_t<uint32_t, 11, 256, 24, kRankBallot, 1>},
+    {64, 8, 384, 16, kRankAtomicOr, passes_t<uint64_t, 8, 384, 16, kRankAtomicOr, 2>},
     {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},
-    {64, 8, 512, 16, kRankMatchAny, passes_t<uint64_t, 8, 512, 16, kRankMatchAny, 1>},
-    {64, 11, 256, 16, kRankBallot, passes_t<uint64_t, 11, 256, 16, kRankBallot, 1>},
-    {64, 11, 256, 16, kRankMatchAny, passes_t<uint64_t, 11, 256, 16, kRankMatchAny, 1>},
+    {64, 8, 256, 12, kRankAtomicOr, passes_t<uint64_t, 8, 256, 12, kRankAtomicOr, 3>},
+    {64, 8, 256, 16, kRankBallot, passes_t<uint64_t, 8, 256, 16, kRankBallot, 2>},
+    {64, 11, 384, 16, kRankBallot, passes_t<uint64_t, 11, 384, 16, kRankBallot, 1>},
     {64, 11, 256, 16, kRankAtomicOr, passes_t<uint64_t, 11, 256, 16, kRankAtomicOr, 1>},
-    {64, 11, 256, 8, kRankMatchAny, passes_t<uint64_t, 11, 256, 8, kRankMatchAny, 2>},
+    {64, 11, 256, 12, kRankAtomicOr, passes_t<uint64_t, 11, 256, 12, kRankAtomicOr, 1>},
+    {64, 11, 256, 16, kRankBallot, passes_t<uint64_t, 11, 256, 16, kRankBallot, 1>},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 

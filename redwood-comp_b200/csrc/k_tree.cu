@@ -11,11 +11,13 @@
 // children once; node 0 (whose range the reference limits to [0, n_brt-1])
 // only writes the entries that sequential execution on a zeroed buffer gives.
 //
-// The fused form computes stages 4, 5 and 6 in one pass: the edge count of
-// node i needs prefix_n[parent[i]], and the parent's prefix length is the
-// larger of the two boundary deltas of i's key range (the parent splits at
-// one end of it), so no second pass over parent[] is needed; the exclusive
-// scan of the counts runs as a decoupled look-back over 256-node tiles.
+// The fused form computes stages 4 and 5 in one pass: the edge count of node i
+// needs prefix_n[parent[i]], and the parent's prefix length is the larger of
+// the two boundary deltas of i's key range (the parent splits at one end of
+// it; when that split is the global minimum the parent is the root, whose
+// prefix_n the reference computes over [0, n_brt-1]), so no second pass over
+// parent[] is needed.  Stage 6 stays a separate single-pass scan: chaining it
+// to the tree's tiles would make every tile wait for the slowest one.
 //
 // Stage 7 follows process_oct_node (func_octree.hpp:28-112) in two kernels:
 // one writes every octree row in full (corner, cell_size, the chain child and
@@ -136,7 +138,17 @@ struct KeyWindow {
   }
 };
 
-// n = n_brt_nodes; keys live in [0, n].
+// delta(a, b) > d, for codes whose top bit is clear (the reference asserts it,
+// func_brt.hpp:30-31): clz(a ^ b) - 1 > d  <=>  a ^ b < 2^(W - 2 - d).  `lim`
+// is that bound (0 when d >= W - 1: never true).
+template <typename K>
+__device__ __forceinline__ K delta_limit(int d) {
+  constexpr int W = KeyTraits<K>::kWordBits;
+  return (d >= 0 && d <= W - 2) ? (K(1) << (W - 2 - d)) : K(0);
+}
+
+// n = n_brt_nodes; keys live in [0, n].  Same searches as func_brt.hpp:45-138
+// (power-of-two divisions written as shifts, delta comparisons as bounds).
 template <typename K, typename KeyAt>
 __device__ __forceinline__ BrtNode brt_node(int i, int n, const KeyAt& key) {
   const K ci = key(i);
@@ -151,27 +163,27 @@ __device__ __forceinline__ BrtNode brt_node(int i, int n, const KeyAt& key) {
   if (i == 0) {
     l = n - 1;
   } else {
-    const int dmin = delta(ci, key(i - d));
+    const K lim = delta_limit<K>(delta(ci, key(i - d)));
     int lmax = 2;
     while ((long long)i + (long long)lmax * d >= 0 && i + lmax * d <= n &&
-           delta(ci, key(i + lmax * d)) > dmin)
+           (ci ^ key(i + lmax * d)) < lim)
       lmax *= 2;
     const int lcut = (d == -1) ? i : n - i;
-    for (int t = lmax / 2, div = 2; t >= 1; div *= 2, t = lmax / div)
-      if (l + t <= lcut && delta(ci, key(i + (l + t) * d)) > dmin) l += t;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+      if (l + t <= lcut && (ci ^ key(i + (l + t) * d)) < lim) l += t;
   }
   BrtNode r;
   r.d = d;
   r.j = i + l * d;
   r.dnode = delta(ci, key(r.j));
+  const K lim = delta_limit<K>(r.dnode);
   int s = 0;
-  const int maxdiv = 1 << log2_ceil_u(uint32_t(l));
+  const int kmax = log2_ceil_u(uint32_t(l));  // divisor runs 2, 4, .. 2^kmax
   const int scut = (d == -1) ? i - 1 : n - i - 1;
-  int div = 2;
-  for (uint32_t t = (uint32_t(l) + 1u) / 2u; div <= maxdiv;
-       div <<= 1, t = (uint32_t(l) + uint32_t(div) - 1u) / uint32_t(div)) {
+  for (int k = 1; k <= kmax; ++k) {
+    const uint32_t t = (uint32_t(l) + (1u << k) - 1u) >> k;
     if (uint32_t(s) + t <= uint32_t(scut) &&
-        delta(ci, key(int(uint32_t(i) + (uint32_t(s) + t) * uint32_t(d)))) > r.dnode)
+        (ci ^ key(int(uint32_t(i) + (uint32_t(s) + t) * uint32_t(d)))) < lim)
       s += int(t);
   }
   r.gamma = i + s * d + min(d, 0);
@@ -218,95 +230,49 @@ __device__ __forceinline__ int fused_edge_count(int i, int n, const KeyAt& key,
   return r.dnode / 3 - parent_prefix / 3;
 }
 
-// Tile: kTreeThreads threads x kTreeNpt consecutive nodes each.
-template <typename K, bool FUSED>
+// One CTA per tile of kTreeTile nodes; node base + q*kTreeThreads + tid for
+// q < kTreeNpt (striped, so every store instruction of a warp is contiguous).
+// With EDGES the kernel also writes edge_count (stages 4 and 5 in one pass);
+// tiles are independent, so no CTA ever waits for another.
+template <typename K, bool EDGES>
 __global__ void __launch_bounds__(kTreeThreads)
     k_radix_tree(const K* __restrict__ codes, Count n_unique_c,
                  uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
                  uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
                  int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
-                 int32_t* __restrict__ edge_offset, uint32_t* __restrict__ desc,
-                 uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
-  constexpr int NW = kTreeThreads / 32, NPT = kTreeNpt, HALO = kTreeHalo;
+                 DevStatus* __restrict__ st) {
+  constexpr int NPT = kTreeNpt, HALO = kTreeHalo;
   constexpr int WIN = kTreeTile + 2 * HALO;
   __shared__ K s_win[WIN];
-  __shared__ uint32_t s_warp[NW + 1];
-  __shared__ uint32_t s_tile, s_excl;
   const uint32_t nu = count_of(n_unique_c);
   if (nu < 3 || nu == RW_COUNT_UNSET) {
     if (blockIdx.x == 0 && threadIdx.x == 0) report_error(st, RW_ERR_DEGENERATE, kSiteTree);
     return;
   }
   const int n = int(nu - 1);
-  const uint32_t n_tiles = (uint32_t(n) + kTreeTile - 1) / kTreeTile;
-  const int root_true_delta = delta(codes[0], codes[n]);
-  const int root_prefix = delta(codes[0], codes[n - 1]);
-  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  uint32_t iter = 0;
-  while (true) {
-    uint32_t tile;
-    if (FUSED) {
-      if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
-      __syncthreads();
-      tile = s_tile;
-    } else {
-      tile = blockIdx.x + iter * gridDim.x;
-      ++iter;
-    }
-    if (tile >= n_tiles) break;
-    const int base = int(tile) * kTreeTile;
-    const int wlo = base - HALO;
-    for (int j = tid; j < WIN; j += kTreeThreads) {
-      const int g = wlo + j;
-      s_win[j] = (g >= 0 && g <= n) ? codes[g] : K(0);
-    }
-    __syncthreads();
-    const KeyWindow<K> key{codes, s_win, wlo, WIN};
-    const int first = base + int(tid) * NPT;
-    int ec[NPT];
-    uint32_t local = 0;
-#pragma unroll
-    for (int q = 0; q < NPT; ++q) {
-      const int i = first + q;
-      ec[q] = 0;
-      if (i < n) {
-        const BrtNode r = brt_node<K>(i, n, key);
-        write_node<K>(i, n, key, r, prefix_n, hl, hr, lc, parents);
-        if (FUSED && i > 0)
-          ec[q] = fused_edge_count<K>(i, n, key, r, root_true_delta, root_prefix);
-      }
-      local += uint32_t(ec[q]);
-    }
-    if (FUSED) {
-      uint32_t total;
-      const uint32_t ex = block_exclusive_scan<kTreeThreads>(local, s_warp, &total);
-      if (warp == 0) {
-        uint32_t excl = 0;
-        if (tile == 0) {
-          if (lane == 0) st_relaxed(desc, kFlagInc | (total << 2));
-        } else {
-          if (lane == 0) st_relaxed(desc + tile, kFlagAgg | (total << 2));
-          excl = warp_lookback(desc, tile, st, kSiteTree);
-          if (lane == 0) st_relaxed(desc + tile, kFlagInc | ((excl + total) << 2));
-        }
-        if (lane == 0) {
-          s_excl = excl;
-          if (tile == n_tiles - 1) st->n_octree_nodes = excl + total;
-        }
-      }
-      __syncthreads();
-      uint32_t run = s_excl + ex;
-#pragma unroll
-      for (int q = 0; q < NPT; ++q) {
-        const int i = first + q;
-        if (i < n) {
-          edge_count[i] = ec[q];
-          edge_offset[i] = int32_t(run);
-        }
-        run += uint32_t(ec[q]);
-      }
-    }
-    __syncthreads();  // the window is reloaded by the next tile
+  const int base = int(blockIdx.x) * kTreeTile;
+  if (base >= n) return;
+  const int wlo = base - HALO;
+  for (int j = threadIdx.x; j < WIN; j += kTreeThreads) {
+    const int g = wlo + j;
+    s_win[j] = (g >= 0 && g <= n) ? codes[g] : K(0);
+  }
+  __syncthreads();
+  const KeyWindow<K> key{codes, s_win, wlo, WIN};
+  int root_true_delta = 0, root_prefix = 0;
+  if (EDGES) {
+    root_true_delta = delta(codes[0], codes[n]);
+    root_prefix = delta(codes[0], codes[n - 1]);
+  }
+#pragma unroll 1
+  for (int q = 0; q < NPT; ++q) {
+    const int i = base + q * kTreeThreads + int(threadIdx.x);
+    if (i >= n) break;
+    const BrtNode r = brt_node<K>(i, n, key);
+    write_node<K>(i, n, key, r, prefix_n, hl, hr, lc, parents);
+    if (EDGES)
+      edge_count[i] =
+          i > 0 ? fused_edge_count<K>(i, n, key, r, root_true_delta, root_prefix) : 0;
   }
 }
 
@@ -538,20 +504,17 @@ cudaError_t unique_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
 
 template <typename K>
 cudaError_t tree_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                   Count nu, bool fused, cudaStream_t s) {
-  const uint32_t tiles = div_up(app.n_input, kTreeTile);
-  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(im, 8)));
+                   Count nu, bool edges, cudaStream_t s) {
+  const uint32_t tiles = std::max(1u, div_up(app.n_input, kTreeTile));
   const K* codes = static_cast<const K*>(app.u_morton_keys);
-  if (fused)
-    k_radix_tree<K, true><<<blocks, kTreeThreads, 0, s>>>(
+  if (edges)
+    k_radix_tree<K, true><<<tiles, kTreeThreads, 0, s>>>(
         codes, nu, app.brt_prefix_n, app.brt_has_leaf_left, app.brt_has_leaf_right,
-        app.brt_left_child, app.brt_parents, app.u_edge_count, app.u_edge_offset,
-        im->d_scan_desc, im->d_tile_ctr + kCtrTree, im->d_status);
+        app.brt_left_child, app.brt_parents, app.u_edge_count, im->d_status);
   else
-    k_radix_tree<K, false><<<blocks, kTreeThreads, 0, s>>>(
+    k_radix_tree<K, false><<<tiles, kTreeThreads, 0, s>>>(
         codes, nu, app.brt_prefix_n, app.brt_has_leaf_left, app.brt_has_leaf_right,
-        app.brt_left_child, app.brt_parents, nullptr, nullptr, nullptr, nullptr,
-        im->d_status);
+        app.brt_left_child, app.brt_parents, nullptr, im->d_status);
   return cudaGetLastError();
 }
 
@@ -587,9 +550,9 @@ cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
 }
 
 cudaError_t launch_radix_tree(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                              Count nu, bool fused, cudaStream_t s) {
-  return app.key_bits == 32 ? tree_t<uint32_t>(app, im, nu, fused, s)
-                            : tree_t<uint64_t>(app, im, nu, fused, s);
+                              Count nu, bool edges, cudaStream_t s) {
+  return app.key_bits == 32 ? tree_t<uint32_t>(app, im, nu, edges, s)
+                            : tree_t<uint64_t>(app, im, nu, edges, s);
 }
 
 cudaError_t launch_edge_count(const rw_tree_app_data& app, rw_tree_im_storage* im,

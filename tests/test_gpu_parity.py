@@ -182,7 +182,10 @@ def test_every_sort_variant_is_exact(rw, oracle):
             app.u_morton_keys.copy_(torch.from_numpy(keys.view(np.int32 if kb == 32 else np.int64)))
             im = rw.ImStorage(n, kb, rb)
             im.set_sort_variant(v["index"])
-            rw.run_stage2(app, im)
+            try:
+                rw.run_stage2(app, im)
+            except rw.RwTreeError as e:
+                raise AssertionError(f"variant {v}: {e}")
             got = app.u_morton_keys_alt.cpu().numpy().view(kt)
             assert np.array_equal(got, np.sort(keys)), (v, n)
         pts = cloud(rw, 30001, "gauss", 5)
