@@ -214,6 +214,21 @@ int rw_tree_generate_points(float* out, uint64_t n, int32_t kind,
                             int32_t n_components, float sigma_lo,
                             float sigma_hi);
 
+/* Stage 3 for callers that cannot allocate GPU memory (a host whose device
+ * memory is all reserved by its own pool, a real-time loop that must not take
+ * the driver's allocation locks, a plugin given only pointers and a stream).
+ * No counterpart in the reference.  Same result as rw_tree_run_stage3: the
+ * unique keys of sorted_keys[0, n) go to unique_keys and their count to
+ * *n_unique (host memory); synchronous on `stream`.  Its scratch is a fixed
+ * array inside the library (about 64 KiB on every GPU that loads it), so it
+ * never allocates; n above RW_NOALLOC_MAX_KEYS is rejected with RW_ERR_ARG.
+ * The first call on each device looks the array's address up (make that call
+ * before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+#define RW_NOALLOC_MAX_KEYS ((uint32_t)1 << 26)
+int rw_tree_unique_noalloc(const void* sorted_keys, void* unique_keys, uint32_t n,
+                           int32_t key_bits, uint32_t* n_unique, rw_stream_t stream);
+
 /* Text of the last CUDA error seen by this thread ("" if none). */
 const char* rw_tree_last_error(void);
 /* Library build tag (kernels compiled for sm_100a). */

@@ -89,6 +89,7 @@ EXPORTS = (
     "rw_tree_last_error", "rw_tree_version", "rw_tree_pipeline_profile",
     "rw_tree_pipeline_kernel_names", "rw_tree_sort_variant_count",
     "rw_tree_sort_variant_info", "rw_tree_im_storage_set_sort_variant",
+    "rw_tree_unique_noalloc",
 )
 
 

@@ -81,6 +81,11 @@ cudaError_t launch_sort_passes(const rw_tree_app_data& app,
                                cudaEvent_t* marks = nullptr);
 cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
                           cudaStream_t s);
+// The unique kernel on caller-given scratch: `desc` holds one word per
+// kUniqueTile keys and, like *tile_ctr and *status, must be zero.
+cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
+                              uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
+                              int num_sms, cudaStream_t s);
 // Stage 4 alone (edges = false) or stages 4 and 5 in one pass (edges = true).
 cudaError_t launch_radix_tree(const rw_tree_app_data& app,
                               rw_tree_im_storage* im, Count n_unique,

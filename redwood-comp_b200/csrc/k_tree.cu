@@ -549,6 +549,22 @@ cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
                             : unique_t<uint64_t>(app, im, s);
 }
 
+cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
+                              uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
+                              int num_sms, cudaStream_t s) {
+  const uint32_t tiles = div_up(n, kUniqueTile);
+  const int blocks = std::max(1, std::min<int>(tiles, num_sms * 8));
+  if (key_bits == 32)
+    k_unique<uint32_t><<<blocks, kUniqueThreads, 0, s>>>(
+        static_cast<const uint32_t*>(sorted), static_cast<uint32_t*>(out), n, desc,
+        tile_ctr, status);
+  else
+    k_unique<uint64_t><<<blocks, kUniqueThreads, 0, s>>>(
+        static_cast<const uint64_t*>(sorted), static_cast<uint64_t*>(out), n, desc,
+        tile_ctr, status);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_radix_tree(const rw_tree_app_data& app, rw_tree_im_storage* im,
                               Count nu, bool edges, cudaStream_t s) {
   return app.key_bits == 32 ? tree_t<uint32_t>(app, im, nu, edges, s)
