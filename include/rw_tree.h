@@ -214,6 +214,63 @@ int rw_tree_generate_points(float* out, uint64_t n, int32_t kind,
                             int32_t n_components, float sigma_lo,
                             float sigma_hi);
 
+/* ---- batched form: many clouds in one pass of launches --------------------
+ * No reference counterpart (the reference builds one cloud per call,
+ * pipe_main_baseline.cpp:55-92).  Clouds are stored back to back: cloud c's
+ * points, keys, radix-tree and edge arrays occupy [point_offset[c],
+ * point_offset[c+1]) of the concatenated buffers, its octree rows
+ * [octree_offset[c], octree_offset[c+1]) with floor(0.6f * n_c) rows per cloud
+ * as AppData allocates.  Every kernel runs once for the whole batch; each
+ * cloud's outputs equal a plain run on that cloud alone. */
+typedef struct rw_tree_batch rw_tree_batch;
+
+typedef struct rw_tree_batch_buffers {
+  float* points;             /* [4 n_total] */
+  void* morton_keys;         /* [n_total] unique keys of each cloud after the run */
+  void* morton_keys_alt;     /* [n_total] sorted keys of each cloud */
+  int32_t* edge_count;       /* [n_total] */
+  int32_t* edge_offset;      /* [n_total] */
+  uint8_t* prefix_n;         /* [n_total] */
+  uint8_t* has_leaf_left;
+  uint8_t* has_leaf_right;
+  int32_t* left_child;
+  int32_t* parents;
+  int32_t* children;         /* [8 octree_rows] */
+  float* corner;             /* [4 octree_rows] */
+  float* cell_size;          /* [octree_rows] */
+  int32_t* child_node_mask;
+  int32_t* child_leaf_mask;
+} rw_tree_batch_buffers;
+
+/* Plans a batch of n_clouds clouds of the given sizes (each >= 1) and
+ * allocates its scratch on the current device.  Cloud c gets
+ * floor(n_c * octree_ratio) octree rows (at least 1), computed in float as
+ * AppData does with its 0.6f (app_data.hpp:13,28); octree_ratio <= 0 means
+ * 0.6f.  Small uniform clouds can need more than 0.6 n rows: their status is
+ * then RW_ERR_CAPACITY, exactly as a plain run with that capacity reports. */
+int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t key_bits,
+                         int32_t radix_bits, float octree_ratio, rw_tree_batch** out);
+int rw_tree_batch_destroy(rw_tree_batch* batch);
+uint32_t rw_tree_batch_total_points(const rw_tree_batch* batch);
+uint32_t rw_tree_batch_octree_rows(const rw_tree_batch* batch);
+/* point_offsets and octree_offsets: [n_clouds + 1] each (either may be NULL). */
+int rw_tree_batch_offsets(const rw_tree_batch* batch, uint32_t* point_offsets,
+                          uint32_t* octree_offsets);
+int rw_tree_batch_set_sort_variant(rw_tree_batch* batch, int32_t idx);
+/* All stages for every cloud, asynchronous on `stream` (capturable). */
+int rw_tree_batch_enqueue(rw_tree_batch* batch, const rw_tree_batch_buffers* bufs,
+                          rw_stream_t stream);
+/* The same through a CUDA graph: captured on the first call for a buffer set
+ * (and again when the buffers or the sort variant change), then replayed. */
+int rw_tree_batch_graph_launch(rw_tree_batch* batch, const rw_tree_batch_buffers* bufs,
+                               rw_stream_t stream);
+/* Waits for the stream; per-cloud n_unique, n_octree_nodes and status
+ * (rw_status: RW_ERR_DEGENERATE / RW_ERR_CAPACITY for that cloud), each
+ * [n_clouds] (NULL to skip).  Returns RW_ERR_TIMEOUT if a device-side wait
+ * gave up. */
+int rw_tree_batch_finish(rw_tree_batch* batch, rw_stream_t stream, uint32_t* n_unique,
+                         uint32_t* n_octree_nodes, int32_t* status);
+
 /* Stage 3 for callers that cannot allocate GPU memory (a host whose device
  * memory is all reserved by its own pool, a real-time loop that must not take
  * the driver's allocation locks, a plugin given only pointers and a stream).

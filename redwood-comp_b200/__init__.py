@@ -70,6 +70,13 @@ class _AppDataC(ctypes.Structure):
     ]
 
 
+class _BatchBufsC(ctypes.Structure):
+    _fields_ = [(name, _vp) for name in (
+        "points", "morton_keys", "morton_keys_alt", "edge_count", "edge_offset", "prefix_n",
+        "has_leaf_left", "has_leaf_right", "left_child", "parents", "children", "corner",
+        "cell_size", "child_node_mask", "child_leaf_mask")]
+
+
 class _HostOutC(ctypes.Structure):
     _fields_ = [(name, _vp) for name in (
         "sorted_keys", "unique_keys", "prefix_n", "has_leaf_left", "has_leaf_right",
@@ -89,7 +96,10 @@ EXPORTS = (
     "rw_tree_last_error", "rw_tree_version", "rw_tree_pipeline_profile",
     "rw_tree_pipeline_kernel_names", "rw_tree_sort_variant_count",
     "rw_tree_sort_variant_info", "rw_tree_im_storage_set_sort_variant",
-    "rw_tree_unique_noalloc",
+    "rw_tree_unique_noalloc", "rw_tree_batch_create", "rw_tree_batch_destroy",
+    "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
+    "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
+    "rw_tree_batch_finish",
 )
 
 
@@ -107,6 +117,8 @@ def lib() -> ctypes.CDLL:
         L.rw_tree_last_error.restype = ctypes.c_char_p
         L.rw_tree_version.restype = ctypes.c_char_p
         L.rw_tree_pipeline_kernel_names.restype = ctypes.c_char_p
+        L.rw_tree_batch_total_points.restype = ctypes.c_uint32
+        L.rw_tree_batch_octree_rows.restype = ctypes.c_uint32
         L.rw_tree_generate_points.argtypes = [
             _vp, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_float,
             ctypes.c_float, ctypes.c_int32, ctypes.c_float, ctypes.c_float]
@@ -351,3 +363,121 @@ def run_host(app: AppData, im: ImStorage, h_points: np.ndarray,
         setattr(ho, name, a.ctypes.data)
     _check(lib().rw_tree_run_host(ctypes.byref(app.c), im.handle, pts.ctypes.data_as(_vp),
                                   ctypes.byref(ho), _stream_handle(stream)), "run_host")
+
+
+class Batch:
+    """Many clouds through the seven stages with one launch per kernel.
+
+    ``clouds``: list of [n_c, 4] float32 host arrays.  Buffers are device
+    tensors concatenated cloud after cloud (the layout of rw_tree.h).
+    """
+
+    def __init__(self, clouds, key_bits: int = 32, radix_bits: int = 0,
+                 octree_ratio: float = 0.6, device: str = "cuda"):
+        import torch
+        sizes = np.array([c.shape[0] for c in clouds], np.uint32)
+        self.n_clouds = len(clouds)
+        self.key_bits = key_bits
+        self.octree_ratio = octree_ratio
+        self._h = _vp()
+        _check(lib().rw_tree_batch_create(sizes.ctypes.data_as(_vp), ctypes.c_uint32(len(sizes)),
+                                          ctypes.c_int32(key_bits), ctypes.c_int32(radix_bits),
+                                          ctypes.c_float(octree_ratio), ctypes.byref(self._h)),
+               "Batch")
+        L = lib()
+        self.n_total = int(L.rw_tree_batch_total_points(self._h))
+        self.oct_rows = int(L.rw_tree_batch_octree_rows(self._h))
+        self.point_offsets = np.zeros(self.n_clouds + 1, np.uint32)
+        self.octree_offsets = np.zeros(self.n_clouds + 1, np.uint32)
+        _check(L.rw_tree_batch_offsets(self._h, self.point_offsets.ctypes.data_as(_vp),
+                                       self.octree_offsets.ctypes.data_as(_vp)), "offsets")
+        n, rows = self.n_total, max(self.oct_rows, 1)
+        kt = torch.int32 if key_bits == 32 else torch.int64
+        dev = torch.device(device)
+        e = lambda *shape, dtype: torch.zeros(*shape, dtype=dtype, device=dev)
+        self.points = e(n, 4, dtype=torch.float32)
+        self.morton_keys = e(n, dtype=kt)
+        self.morton_keys_alt = e(n, dtype=kt)
+        self.edge_count = e(n, dtype=torch.int32)
+        self.edge_offset = e(n, dtype=torch.int32)
+        self.prefix_n = e(n, dtype=torch.uint8)
+        self.has_leaf_left = e(n, dtype=torch.uint8)
+        self.has_leaf_right = e(n, dtype=torch.uint8)
+        self.left_child = e(n, dtype=torch.int32)
+        self.parents = e(n, dtype=torch.int32)
+        self.children = e(rows, 8, dtype=torch.int32)
+        self.corner = e(rows, 4, dtype=torch.float32)
+        self.cell_size = e(rows, dtype=torch.float32)
+        self.child_node_mask = e(rows, dtype=torch.int32)
+        self.child_leaf_mask = e(rows, dtype=torch.int32)
+        self.set_points(clouds)
+        c = _BatchBufsC()
+        for name, _ in _BatchBufsC._fields_:
+            setattr(c, name, getattr(self, name).data_ptr())
+        self._c = c
+        self.n_unique = np.zeros(self.n_clouds, np.uint32)
+        self.n_octree_nodes = np.zeros(self.n_clouds, np.uint32)
+        self.status = np.zeros(self.n_clouds, np.int32)
+
+    def capacity(self, c: int) -> int:
+        return int(self.octree_offsets[c + 1] - self.octree_offsets[c])
+
+    def set_points(self, clouds) -> None:
+        import torch
+        host = np.concatenate([np.ascontiguousarray(c, np.float32).reshape(-1, 4) for c in clouds])
+        self.points.copy_(torch.from_numpy(host))
+
+    def set_sort_variant(self, idx: int) -> None:
+        _check(lib().rw_tree_batch_set_sort_variant(self._h, idx), "batch_set_sort_variant")
+
+    def enqueue(self, graph: bool = True, stream=None) -> None:
+        fn = lib().rw_tree_batch_graph_launch if graph else lib().rw_tree_batch_enqueue
+        _check(fn(self._h, ctypes.byref(self._c), _stream_handle(stream)), "batch_enqueue")
+
+    def finish(self, stream=None) -> None:
+        _check(lib().rw_tree_batch_finish(
+            self._h, _stream_handle(stream), self.n_unique.ctypes.data_as(_vp),
+            self.n_octree_nodes.ctypes.data_as(_vp), self.status.ctypes.data_as(_vp)),
+            "batch_finish")
+
+    def run(self, graph: bool = True, stream=None) -> None:
+        self.enqueue(graph, stream)
+        self.finish(stream)
+
+    def results(self, c: int) -> dict:
+        """Cloud c's outputs, host copies cut to their meaningful lengths."""
+        p0, p1 = int(self.point_offsets[c]), int(self.point_offsets[c + 1])
+        r0 = int(self.octree_offsets[c])
+        u = int(self.n_unique[c])
+        b = u - 1
+        m = int(self.n_octree_nodes[c])
+        kv = np.uint32 if self.key_bits == 32 else np.uint64
+        return {
+            "sorted_keys": self.morton_keys_alt[p0:p1].cpu().numpy().view(kv),
+            "unique_keys": self.morton_keys[p0:p0 + u].cpu().numpy().view(kv),
+            "n_unique": u,
+            "prefix_n": self.prefix_n[p0:p0 + b].cpu().numpy(),
+            "has_leaf_left": self.has_leaf_left[p0:p0 + b].cpu().numpy(),
+            "has_leaf_right": self.has_leaf_right[p0:p0 + b].cpu().numpy(),
+            "left_child": self.left_child[p0:p0 + b].cpu().numpy(),
+            "parents": self.parents[p0:p0 + b].cpu().numpy(),
+            "edge_count": self.edge_count[p0:p0 + b].cpu().numpy(),
+            "edge_offset": self.edge_offset[p0:p0 + b].cpu().numpy(),
+            "n_octree_nodes": m,
+            "children": self.children[r0:r0 + m].cpu().numpy(),
+            "corner": self.corner[r0:r0 + m].cpu().numpy(),
+            "cell_size": self.cell_size[r0:r0 + m].cpu().numpy(),
+            "child_node_mask": self.child_node_mask[r0:r0 + m].cpu().numpy(),
+            "child_leaf_mask": self.child_leaf_mask[r0:r0 + m].cpu().numpy(),
+        }
+
+    def close(self) -> None:
+        if self._h:
+            lib().rw_tree_batch_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

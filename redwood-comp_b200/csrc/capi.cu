@@ -67,9 +67,61 @@ int check(const rw_tree_app_data* app, const rw_tree_im_storage* im, unsigned ne
   return RW_OK;
 }
 
-// Zero parts of the scratch's zero region.
-int clear_status(rw_tree_im_storage* im, cudaStream_t s) {
-  RW_CUDA(cudaMemsetAsync(im->d_status, 0, sizeof(rwt::DevStatus), s));
+rwt::Bufs bufs_of(const rw_tree_app_data& a, const rw_tree_im_storage* im) {
+  rwt::Bufs b;
+  b.key_bits = a.key_bits;
+  b.min_coord = a.min_coord;
+  b.range = a.range;
+  b.points = reinterpret_cast<const float4*>(a.u_input_points);
+  b.keys = a.u_morton_keys;
+  b.alt = a.u_morton_keys_alt;
+  b.tmp = im->d_tmp_keys;
+  b.prefix_n = a.brt_prefix_n;
+  b.hl = a.brt_has_leaf_left;
+  b.hr = a.brt_has_leaf_right;
+  b.lc = a.brt_left_child;
+  b.parents = a.brt_parents;
+  b.edge_count = a.u_edge_count;
+  b.edge_offset = a.u_edge_offset;
+  b.children = a.oct_children;
+  b.corner = reinterpret_cast<float4*>(a.oct_corner);
+  b.cell_size = a.oct_cell_size;
+  b.node_mask = a.oct_child_node_mask;
+  b.leaf_mask = a.oct_child_leaf_mask;
+  return b;
+}
+
+rwt::Scratch scratch_of(const rw_tree_im_storage* im) {
+  rwt::Scratch sc;
+  sc.num_sms = im->num_sms;
+  sc.radix_bits = im->radix_bits;
+  sc.passes = im->passes;
+  sc.sort_variant = im->sort_variant;
+  sc.ghist = im->d_ghist;
+  sc.sort_desc = im->d_sort_desc;
+  sc.sort_rows = im->sort_tiles + 1;
+  sc.unique_desc = im->d_unique_desc;
+  sc.scan_desc = im->d_scan_desc;
+  sc.tile_ctr = im->d_tile_ctr;
+  sc.status = im->d_status;
+  return sc;
+}
+
+rwt::Plan plan_of(const rw_tree_app_data& a, const rw_tree_im_storage* im) {
+  return rwt::single_plan(a.n_input, a.oct_capacity, im->d_status,
+                          rwt::sort_variant_tile(im->sort_variant));
+}
+
+// Device status := the host's counts of `app`, error word cleared (for the
+// per-stage calls whose kernels read the counts on the device).
+int upload_counts(const rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s) {
+  RW_CUDA(cudaStreamSynchronize(s));  // the pinned mirror may still be in use
+  im->h_status->n_unique = app->n_unique;
+  im->h_status->n_octree_nodes = app->n_octree_nodes;
+  im->h_status->err = 0;
+  im->h_status->err_site = 0;
+  RW_CUDA(cudaMemcpyAsync(im->d_status, im->h_status, sizeof(rwt::DevStatus),
+                          cudaMemcpyHostToDevice, s));
   return RW_OK;
 }
 
@@ -94,6 +146,10 @@ int sync_status(rw_tree_im_storage* im, cudaStream_t s) {
 }
 
 }  // namespace
+
+namespace rwt {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace rwt
 
 extern "C" {
 
@@ -223,7 +279,8 @@ int rw_tree_run_stage1(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {
   if (int rc = check(app, im, kPoints | kKeys)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  RW_CUDA(rwt::launch_morton(*app, im, false, s));
+  RW_CUDA(rwt::launch_keys(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), true, false,
+                           s));
   RW_CUDA(cudaStreamSynchronize(s));
   return RW_OK;
 }
@@ -234,8 +291,11 @@ int rw_tree_run_stage2(rw_tree_app_data* app, rw_tree_im_storage* im,
   if (int rc = check(app, im, kKeys | kAlt)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = clear_all(im, s)) return rc;
-  RW_CUDA(rwt::launch_histogram(*app, im, s));
-  RW_CUDA(rwt::launch_sort_passes(*app, im, s));
+  const auto b = bufs_of(*app, im);
+  const auto sc = scratch_of(im);
+  const auto pl = plan_of(*app, im);
+  RW_CUDA(rwt::launch_keys(b, sc, pl, false, true, s));
+  RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s));
   return sync_status(im, s);
 }
 
@@ -245,7 +305,7 @@ int rw_tree_run_stage3(rw_tree_app_data* app, rw_tree_im_storage* im,
   if (int rc = check(app, im, kKeys | kAlt)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = clear_all(im, s)) return rc;
-  RW_CUDA(rwt::launch_unique(*app, im, s));
+  RW_CUDA(rwt::launch_unique(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
   if (int rc = sync_status(im, s)) return rc;
   app->n_unique = im->h_status->n_unique;
   app->n_brt_nodes = app->n_unique - 1;
@@ -257,10 +317,11 @@ int rw_tree_run_stage4(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {
   if (int rc = check(app, im, kKeys | kBrt)) return rc;
   if (app->n_unique == RW_COUNT_UNSET) return RW_ERR_NOT_READY;
-  if (app->n_unique < 3) return RW_ERR_DEGENERATE;
+  if (app->n_unique < 3 || app->n_unique > app->n_input) return RW_ERR_DEGENERATE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (int rc = clear_status(im, s)) return rc;
-  RW_CUDA(rwt::launch_radix_tree(*app, im, rwt::Count{nullptr, app->n_unique}, false, s));
+  if (int rc = upload_counts(app, im, s)) return rc;
+  RW_CUDA(rwt::launch_radix_tree(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), false,
+                                 s));
   return sync_status(im, s);
 }
 
@@ -269,11 +330,11 @@ int rw_tree_run_stage5(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {
   if (int rc = check(app, im, kBrt | kEdge)) return rc;
   if (app->n_unique == RW_COUNT_UNSET) return RW_ERR_NOT_READY;
-  if (app->n_unique < 3) return RW_ERR_DEGENERATE;
+  if (app->n_unique < 3 || app->n_unique > app->n_input) return RW_ERR_DEGENERATE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  RW_CUDA(rwt::launch_edge_count(*app, im, rwt::Count{nullptr, app->n_unique}, s));
-  RW_CUDA(cudaStreamSynchronize(s));
-  return RW_OK;
+  if (int rc = upload_counts(app, im, s)) return rc;
+  RW_CUDA(rwt::launch_edge_count(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
+  return sync_status(im, s);
 }
 
 // ---- stage 6: exclusive scan (cu_dispatcher.cu:672-686) -----------------------
@@ -281,10 +342,11 @@ int rw_tree_run_stage6(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {
   if (int rc = check(app, im, kEdge)) return rc;
   if (app->n_unique == RW_COUNT_UNSET) return RW_ERR_NOT_READY;
-  if (app->n_unique < 3) return RW_ERR_DEGENERATE;
+  if (app->n_unique < 3 || app->n_unique > app->n_input) return RW_ERR_DEGENERATE;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = clear_all(im, s)) return rc;
-  RW_CUDA(rwt::launch_edge_scan(*app, im, rwt::Count{nullptr, app->n_unique}, s));
+  if (int rc = upload_counts(app, im, s)) return rc;
+  RW_CUDA(rwt::launch_edge_scan(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
   if (int rc = sync_status(im, s)) return rc;
   app->n_octree_nodes = im->h_status->n_octree_nodes;
   return RW_OK;
@@ -296,12 +358,11 @@ int rw_tree_run_stage7(rw_tree_app_data* app, rw_tree_im_storage* im,
   if (int rc = check(app, im, kKeys | kBrt | kEdge | kOct)) return rc;
   if (app->n_unique == RW_COUNT_UNSET || app->n_octree_nodes == RW_COUNT_UNSET)
     return RW_ERR_NOT_READY;
-  if (app->n_unique < 3) return RW_ERR_DEGENERATE;
+  if (app->n_unique < 3 || app->n_unique > app->n_input) return RW_ERR_DEGENERATE;
   if (uint64_t(app->n_octree_nodes) + 1 > app->oct_capacity) return RW_ERR_CAPACITY;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (int rc = clear_status(im, s)) return rc;
-  RW_CUDA(rwt::launch_octree(*app, im, rwt::Count{nullptr, app->n_unique},
-                             rwt::Count{nullptr, app->n_octree_nodes}, s));
+  if (int rc = upload_counts(app, im, s)) return rc;
+  RW_CUDA(rwt::launch_octree(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
   return sync_status(im, s);
 }
 
@@ -318,20 +379,21 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
     return ev ? cudaEventRecord(ev[k++], s) : cudaSuccess;
   };
   if (int rc = clear_all(im, s)) return rc;
+  const auto b = bufs_of(*app, im);
+  const auto sc = scratch_of(im);
+  const auto pl = plan_of(*app, im);
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_morton(*app, im, true, s));
+  RW_CUDA(rwt::launch_keys(b, sc, pl, true, true, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_sort_passes(*app, im, s, ev ? ev + k : nullptr));
+  RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s, ev ? ev + k : nullptr));
   if (ev) k += 1 + im->passes;
-  RW_CUDA(rwt::launch_unique(*app, im, s));
+  RW_CUDA(rwt::launch_unique(b, sc, pl, s));
   RW_CUDA(mark());
-  const rwt::Count nu{&im->d_status->n_unique, 0};
-  const rwt::Count nm{&im->d_status->n_octree_nodes, 0};
-  RW_CUDA(rwt::launch_radix_tree(*app, im, nu, true, s));
+  RW_CUDA(rwt::launch_radix_tree(b, sc, pl, true, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_edge_scan(*app, im, nu, s));
+  RW_CUDA(rwt::launch_edge_scan(b, sc, pl, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_octree(*app, im, nu, nm, s, ev ? ev + k : nullptr));
+  RW_CUDA(rwt::launch_octree(b, sc, pl, s, ev ? ev + k : nullptr));
   if (ev) k += 2;
   RW_CUDA(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(rwt::DevStatus),
                           cudaMemcpyDeviceToHost, s));

@@ -108,21 +108,62 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* total) {
   return out;
 }
 
+// ---------------------------------------------------------------------------
+// Segments: a batch of independent point clouds stored back to back.  A plain
+// run is one segment.  Every kernel walks a tile map: segment c owns the tiles
+// [toff[c], toff[c+1]) of that kernel's tile size.
+// ---------------------------------------------------------------------------
+struct SegTable {
+  uint32_t count;       // segments
+  uint32_t total;       // points over all segments
+  const uint32_t* off;  // [count + 1] point offsets (device); null when count == 1
+};
+
+struct TileMap {
+  uint32_t n_tiles;      // tiles over all segments
+  const uint32_t* toff;  // [count + 1] tile offsets (device); null when count == 1
+};
+
+__device__ __forceinline__ uint32_t seg_begin(const SegTable& s, uint32_t c) {
+  return s.off ? s.off[c] : 0u;
+}
+__device__ __forceinline__ uint32_t seg_size(const SegTable& s, uint32_t c) {
+  return s.off ? s.off[c + 1] - s.off[c] : s.total;
+}
+// Segment of global tile t and its first tile.
+__device__ __forceinline__ uint32_t tile_segment(const SegTable& s, const TileMap& m,
+                                                 uint32_t t, uint32_t* first_tile) {
+  if (!m.toff) {
+    *first_tile = 0;
+    return 0;
+  }
+  uint32_t lo = 0, hi = s.count;  // toff[lo] <= t < toff[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (m.toff[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  *first_tile = m.toff[lo];
+  return lo;
+}
+
 // Warp-cooperative look-back for a single-value chained scan.  Called by one
-// whole warp of the tile `tile` (> 0).  desc[t] holds tile t's descriptor.
-// Returns the exclusive prefix of `tile` (sum of all earlier tiles).  On a
-// timeout it reports the error and returns 0.
+// whole warp of the tile `tile` (> first).  desc[t] holds tile t's descriptor;
+// the chain starts at tile `first` (the segment's first tile).  Returns the
+// exclusive prefix of `tile` within its segment.  On a timeout it reports the
+// error and returns 0.
 __device__ __forceinline__ uint32_t warp_lookback(const uint32_t* desc,
                                                   uint32_t tile,
                                                   DevStatus* st,
-                                                  uint32_t site) {
+                                                  uint32_t site,
+                                                  uint32_t first = 0) {
   const uint32_t lane = lane_id();
   uint32_t excl = 0;
   int64_t hi = (int64_t)tile - 1;  // nearest predecessor still to read
   uint32_t spin = 0;
   while (true) {
     const int64_t idx = hi - (int64_t)lane;
-    const uint32_t d = idx >= 0 ? ld_relaxed(desc + idx) : (kFlagInc);
+    const uint32_t d = idx >= (int64_t)first ? ld_relaxed(desc + idx) : (kFlagInc);
     const uint32_t f = d & kFlagMask;
     const uint32_t inc_mask = __ballot_sync(0xffffffffu, f == kFlagInc);
     const uint32_t bad_mask = __ballot_sync(0xffffffffu, f == 0u);

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "common.cuh"
 #include "rw_tree.h"
 
@@ -44,14 +46,16 @@ namespace rwt {
 enum : int { kCtrUnique = 0, kCtrScan = 1, kCtrTree = 2, kCtrSortBase = 4,
              kCounters = 32 };
 
-// Tiles for the single-value chained scans (unique, edge-offset scan, fused
-// radix tree).
+// Tile sizes of the kernels (points or nodes per tile).
+constexpr uint32_t kPointTile = 4096;  // Morton / histogram
 constexpr uint32_t kUniqueThreads = 256, kUniqueKpt = 16;
 constexpr uint32_t kUniqueTile = kUniqueThreads * kUniqueKpt;
 constexpr uint32_t kScanThreads = 256, kScanKpt = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanKpt;
 constexpr int kTreeThreads = 256, kTreeNpt = 4, kTreeHalo = 256;
 constexpr uint32_t kTreeTile = kTreeThreads * kTreeNpt;
+constexpr int kOctThreads = 256, kOctNpt = 4;
+constexpr uint32_t kOctTile = kOctThreads * kOctNpt;
 
 inline uint32_t div_up(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 
@@ -61,43 +65,91 @@ struct Count {
   uint32_t value;
 };
 
+// Device buffers of one pipeline run: one AppData, or a batch of clouds
+// stored back to back (octree rows at per-cloud row offsets).
+struct Bufs {
+  int key_bits = 32;
+  float min_coord = 0.0f, range = 1024.0f;
+  const float4* points = nullptr;
+  void* keys = nullptr;
+  void* alt = nullptr;
+  void* tmp = nullptr;  // ping-pong buffer of the sort
+  uint8_t* prefix_n = nullptr;
+  uint8_t* hl = nullptr;
+  uint8_t* hr = nullptr;
+  int32_t* lc = nullptr;
+  int32_t* parents = nullptr;
+  int32_t* edge_count = nullptr;
+  int32_t* edge_offset = nullptr;
+  int32_t* children = nullptr;
+  float4* corner = nullptr;
+  float* cell_size = nullptr;
+  int32_t* node_mask = nullptr;
+  int32_t* leaf_mask = nullptr;
+};
+
+// Scratch: histograms, descriptors, tickets, status.
+struct Scratch {
+  int num_sms = 148;
+  int radix_bits = 8;
+  int passes = 4;
+  int sort_variant = 0;
+  uint32_t* ghist = nullptr;      // [segments][passes][radix]
+  uint32_t* sort_desc = nullptr;  // [passes][sort_rows][radix]
+  uint32_t sort_rows = 0;         // rows per pass: sort tiles + segments
+  uint32_t* unique_desc = nullptr;
+  uint32_t* scan_desc = nullptr;
+  uint32_t* tile_ctr = nullptr;
+  DevStatus* status = nullptr;
+};
+
+// Segments and the tile map of every kernel, plus per-segment results.
+struct Plan {
+  SegTable seg{};
+  TileMap point_map{}, sort_map{}, unique_map{}, tree_map{}, scan_map{}, node_map{};
+  uint32_t* n_unique = nullptr;  // [segments]
+  uint32_t* n_octree = nullptr;  // [segments]
+  int32_t* seg_err = nullptr;    // [segments] first error of each segment
+  const uint32_t* oct_off = nullptr;  // [segments + 1] octree row offsets
+  uint32_t oct_capacity = 0;          // rows when there is one segment
+};
+
 // ---- onesweep variant menu (k_keys.cu) --------------------------------------
 uint32_t sort_tile_for(int key_bits, int radix_bits);
+uint32_t sort_variant_tile(int idx);
 int sort_variant_count();
 int sort_variant_info(int idx, int* key_bits, int* radix_bits, int* threads, int* kpt,
                       int* rank);
 int default_sort_variant(int key_bits, int radix_bits);
 
 // ---- launchers (each returns the launch's cudaError_t) --------------------
-
-cudaError_t launch_morton(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          bool with_histogram, cudaStream_t s);
-cudaError_t launch_histogram(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                             cudaStream_t s);
-// `marks`, when given, gets one event recorded after sort_init and after each
-// pass (profiling only).
-cudaError_t launch_sort_passes(const rw_tree_app_data& app,
-                               rw_tree_im_storage* im, cudaStream_t s,
-                               cudaEvent_t* marks = nullptr);
-cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          cudaStream_t s);
+// Stage 1 (encode) and/or the sort's digit histograms (hist).
+cudaError_t launch_keys(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode,
+                        bool hist, cudaStream_t s);
+// Init rows + every pass; `marks`, when given, gets one event after the init
+// kernel and one after each pass (profiling only).
+cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,
+                               cudaStream_t s, cudaEvent_t* marks = nullptr);
+cudaError_t launch_unique(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
 // The unique kernel on caller-given scratch: `desc` holds one word per
 // kUniqueTile keys and, like *tile_ctr and *status, must be zero.
 cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
                               uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
                               int num_sms, cudaStream_t s);
 // Stage 4 alone (edges = false) or stages 4 and 5 in one pass (edges = true).
-cudaError_t launch_radix_tree(const rw_tree_app_data& app,
-                              rw_tree_im_storage* im, Count n_unique,
-                              bool edges, cudaStream_t s);
-cudaError_t launch_edge_count(const rw_tree_app_data& app,
-                              rw_tree_im_storage* im, Count n_unique,
+cudaError_t launch_radix_tree(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
                               cudaStream_t s);
-cudaError_t launch_edge_scan(const rw_tree_app_data& app,
-                             rw_tree_im_storage* im, Count n_unique,
-                             cudaStream_t s);
-cudaError_t launch_octree(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          Count n_unique, Count n_octree, cudaStream_t s,
+cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
+                              cudaStream_t s);
+cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
+cudaError_t launch_octree(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
                           cudaEvent_t* marks = nullptr);
+
+// Text returned by rw_tree_last_error (this thread).
+void set_last_error(const std::string& msg);
+
+// One-segment plan for n points (tile maps computed arithmetically); counts
+// and errors go to `status`.
+Plan single_plan(uint32_t n, uint32_t oct_capacity, DevStatus* status, uint32_t sort_tile);
 
 }  // namespace rwt

@@ -24,72 +24,79 @@ namespace rwt {
 // stage 1
 // ---------------------------------------------------------------------------
 
-template <typename K, int D, bool HIST>
+// Points are walked in tiles of kPointTile that never straddle two segments;
+// each CTA takes a contiguous run of tiles, so with HIST its shared-memory
+// histograms are flushed to the segment's global ones only when the segment
+// changes.  ghist: [segments][passes][RADIX].
+template <typename K, int D, bool HIST, bool ENCODE>
 __global__ void __launch_bounds__(256)
-    k_morton(const float4* __restrict__ pts, K* __restrict__ keys, uint32_t n,
-             float min_coord, float range, uint32_t* __restrict__ ghist,
-             int passes) {
-  constexpr int RADIX = 1 << D;
-  extern __shared__ uint32_t s_hist[];  // [passes][RADIX] when HIST
-  if (HIST) {
-    for (int i = threadIdx.x; i < passes * RADIX; i += blockDim.x) s_hist[i] = 0;
-    __syncthreads();
-  }
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const float4 p = __ldcs(pts + i);
-    const K k = encode<K>(p.x, p.y, p.z, min_coord, range);
-    keys[i] = k;
-    if (HIST) {
-      for (int ps = 0; ps < passes; ++ps)
-        atomicAdd(&s_hist[ps * RADIX + int((k >> (ps * D)) & K(RADIX - 1))], 1u);
-    }
-  }
-  if (HIST) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < passes * RADIX; i += blockDim.x) {
-      const uint32_t c = s_hist[i];
-      if (c) atomicAdd(&ghist[i], c);
-    }
-  }
-}
-
-// Digit histograms of all passes from keys already in memory (stage 2 called
-// on its own).
-template <typename K, int D>
-__global__ void __launch_bounds__(256)
-    k_histogram(const K* __restrict__ keys, uint32_t n,
+    k_keys_pass(const float4* __restrict__ pts, K* __restrict__ keys, SegTable seg,
+                TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
                 uint32_t* __restrict__ ghist, int passes) {
   constexpr int RADIX = 1 << D;
-  extern __shared__ uint32_t s_hist[];
-  for (int i = threadIdx.x; i < passes * RADIX; i += blockDim.x) s_hist[i] = 0;
-  __syncthreads();
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const K k = keys[i];
-    for (int ps = 0; ps < passes; ++ps)
-      atomicAdd(&s_hist[ps * RADIX + int((k >> (ps * D)) & K(RADIX - 1))], 1u);
+  extern __shared__ uint32_t s_hist[];  // [passes][RADIX] when HIST
+  const int nh = passes * RADIX;
+  if (HIST) {
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < passes * RADIX; i += blockDim.x) {
-    const uint32_t c = s_hist[i];
-    if (c) atomicAdd(&ghist[i], c);
+  const uint32_t t0 = blockIdx.x * tiles_per_cta;
+  const uint32_t t1 = min(t0 + tiles_per_cta, map.n_tiles);
+  uint32_t cur = 0xffffffffu;
+  auto flush = [&](uint32_t c) {
+    __syncthreads();
+    uint32_t* g = ghist + size_t(c) * nh;
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) {
+      const uint32_t v = s_hist[i];
+      if (v) atomicAdd(&g[i], v);
+      s_hist[i] = 0;
+    }
+    __syncthreads();
+  };
+  for (uint32_t t = t0; t < t1; ++t) {
+    uint32_t first;
+    const uint32_t c = tile_segment(seg, map, t, &first);
+    if (HIST && c != cur && cur != 0xffffffffu) flush(cur);
+    cur = c;
+    const uint32_t sb = seg_begin(seg, c);
+    const uint32_t lo = sb + (t - first) * kPointTile;
+    const uint32_t hi = min(lo + kPointTile, sb + seg_size(seg, c));
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      K k;
+      if (ENCODE) {
+        const float4 p = __ldcs(pts + i);
+        k = encode<K>(p.x, p.y, p.z, min_coord, range);
+        keys[i] = k;
+      } else {
+        k = keys[i];
+      }
+      if (HIST) {
+        for (int ps = 0; ps < passes; ++ps)
+          atomicAdd(&s_hist[ps * RADIX + int((k >> (ps * D)) & K(RADIX - 1))], 1u);
+      }
+    }
   }
+  if (HIST && cur != 0xffffffffu) flush(cur);
 }
 
-// One block per pass: exclusive scan of the pass's digit histogram, stored as
-// the inclusive descriptor of the virtual tile before tile 0.
+// One block per (segment, pass): exclusive scan of the segment's digit
+// histogram, stored as the inclusive descriptor of the virtual tile before the
+// segment's first tile.  Values are absolute positions (segment start added).
+// Descriptor rows of a pass: segment c's init row is toff[c] + c, its tile j
+// uses row toff[c] + c + 1 + j.
 template <int D>
 __global__ void __launch_bounds__(256)
     k_sort_init(const uint32_t* __restrict__ ghist, uint32_t* __restrict__ desc,
-                uint32_t tiles_plus_one) {
+                SegTable seg, TileMap map, int passes, uint32_t rows_per_pass) {
   constexpr int RADIX = 1 << D;
   constexpr int R = (RADIX + 255) / 256;
   static_assert(R * 256 >= RADIX, "every digit needs an offset");
   __shared__ uint32_t s_warp[9];
-  const int pass = blockIdx.x;
-  const uint32_t* h = ghist + pass * RADIX;
-  uint32_t* row0 = desc + size_t(pass) * tiles_plus_one * RADIX;
+  const uint32_t c = blockIdx.x / passes;
+  const int pass = int(blockIdx.x % passes);
+  const uint32_t* h = ghist + (size_t(c) * passes + pass) * RADIX;
+  const uint32_t init_row = (map.toff ? map.toff[c] : 0u) + c;
+  uint32_t* row0 = desc + (size_t(pass) * rows_per_pass + init_row) * RADIX;
   uint32_t v[R];
   uint32_t local = 0;
   const int first = threadIdx.x * R;
@@ -99,7 +106,7 @@ __global__ void __launch_bounds__(256)
     local += v[r];
   }
   uint32_t total;
-  uint32_t run = block_exclusive_scan<256>(local, s_warp, &total);
+  uint32_t run = seg_begin(seg, c) + block_exclusive_scan<256>(local, s_warp, &total);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     if (first + r < RADIX) row0[first + r] = kFlagInc | (run << 2);
@@ -169,7 +176,7 @@ struct BinCfg {
 // exclusive digit offsets (k_sort_init), rows 1.. zero.
 template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
-    k_binning(const K* __restrict__ in, K* __restrict__ out, uint32_t n,
+    k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
               uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
@@ -192,7 +199,12 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
   __syncthreads();
   const uint32_t tile = s_misc[0];
-  const uint32_t base = tile * TILE;
+  uint32_t first_tile;
+  const uint32_t segc = tile_segment(seg, map, tile, &first_tile);
+  const uint32_t base = seg_begin(seg, segc) + (tile - first_tile) * TILE;
+  const uint32_t n = seg_begin(seg, segc) + seg_size(seg, segc);  // end of the segment
+  const uint32_t row = tile + segc + 1;       // this tile's descriptor row
+  const uint32_t init_row = first_tile + segc;  // the segment's inclusive row
 
   // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
   K keys[KPT];
@@ -240,7 +252,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
   // per digit: exclusive scan over warps, publish the tile aggregate, then
   // look back at once so the inclusive prefix is out as early as possible
-  uint32_t* drow = desc + size_t(tile + 1) * RADIX;
+  uint32_t* drow = desc + size_t(row) * RADIX;
   for (int d = tid; d < RADIX; d += THREADS) {
     uint32_t run = 0;
 #pragma unroll
@@ -255,13 +267,14 @@ __global__ void __launch_bounds__(THREADS, MINB)
   for (int d = tid; d < RADIX; d += THREADS) {
     // walk back 4 descriptors per round trip; row 0 is always inclusive
     uint32_t excl = 0;
-    int64_t k = tile;  // row k holds tile k-1's descriptor (row 0: global)
+    int64_t k = row - 1;  // the predecessor's row; the init row is inclusive
     uint32_t spin = 0;
     while (true) {
       uint32_t v[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        v[q] = k - q >= 0 ? ld_relaxed(desc + size_t(k - q) * RADIX + d) : kFlagInc;
+        v[q] = k - q >= int64_t(init_row) ? ld_relaxed(desc + size_t(k - q) * RADIX + d)
+                                          : kFlagInc;
       bool done = false;
       int used = 0;
 #pragma unroll
@@ -313,7 +326,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     const K k = s_keys[p];
     const uint32_t dig = uint32_t(k >> shift) & (RADIX - 1);
     const uint32_t dst = s_gofs[dig] + p;
-    if (dst < n) out[dst] = k;  // always true unless a look-back gave up
+    if (dst < seg.total) out[dst] = k;  // always true unless a look-back gave up
   }
 }
 
@@ -324,64 +337,55 @@ __global__ void __launch_bounds__(THREADS, MINB)
 namespace {
 
 template <typename K, int D>
-cudaError_t morton_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                     bool hist, cudaStream_t s) {
-  const uint32_t n = app.n_input;
-  const int blocks = std::max(1, std::min<int>(div_up(n, 256), im->num_sms * 8));
-  const float4* pts = reinterpret_cast<const float4*>(app.u_input_points);
-  K* keys = static_cast<K*>(app.u_morton_keys);
-  if (hist) {
-    const size_t smem = size_t(im->passes) * (1u << D) * 4;
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_morton<K, D, true>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    k_morton<K, D, true><<<blocks, 256, smem, s>>>(
-        pts, keys, n, app.min_coord, app.range, im->d_ghist, im->passes);
-  } else {
-    k_morton<K, D, false><<<blocks, 256, 0, s>>>(pts, keys, n, app.min_coord,
-                                                 app.range, nullptr, 0);
-  }
-  return cudaGetLastError();
-}
-
-template <typename K, int D>
-cudaError_t histogram_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                        cudaStream_t s) {
-  const uint32_t n = app.n_input;
-  const int blocks = std::max(1, std::min<int>(div_up(n, 256), im->num_sms * 8));
-  const size_t smem = size_t(im->passes) * (1u << D) * 4;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_histogram<K, D>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  k_histogram<K, D><<<blocks, 256, smem, s>>>(
-      static_cast<const K*>(app.u_morton_keys), n, im->d_ghist, im->passes);
+cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode,
+                   bool hist, cudaStream_t s) {
+  const uint32_t tiles = pl.point_map.n_tiles;
+  if (tiles == 0) return cudaSuccess;
+  const uint32_t ctas = std::max(1u, std::min<uint32_t>(tiles, uint32_t(sc.num_sms) * 8));
+  const uint32_t per = div_up(tiles, ctas);
+  const uint32_t grid = div_up(tiles, per);
+  const size_t smem = hist ? size_t(sc.passes) * (1u << D) * 4 : 0;
+  K* keys = static_cast<K*>(b.keys);
+#define RWT_KEYS_LAUNCH(H, E)                                                        \
+  do {                                                                               \
+    auto kern = k_keys_pass<K, D, H, E>;                                             \
+    if (smem > 48 * 1024)                                                            \
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+    kern<<<grid, 256, smem, s>>>(b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
+                                 b.range, sc.ghist, sc.passes);                      \
+  } while (0)
+  if (encode && hist) RWT_KEYS_LAUNCH(true, true);
+  else if (encode) RWT_KEYS_LAUNCH(false, true);
+  else RWT_KEYS_LAUNCH(true, false);
+#undef RWT_KEYS_LAUNCH
   return cudaGetLastError();
 }
 
 template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
-cudaError_t passes_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                     cudaStream_t s, cudaEvent_t* marks) {
+cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
+                     cudaEvent_t* marks) {
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
   auto kern = k_binning<K, D, THREADS, KPT, RANK, MINB>;
-  const uint32_t n = app.n_input;
-  const uint32_t tiles = div_up(n, C::TILE);
-  const uint32_t rows = im->sort_tiles + 1;
-  if (tiles > im->sort_tiles) return cudaErrorInvalidValue;
-  k_sort_init<D><<<im->passes, 256, 0, s>>>(im->d_ghist, im->d_sort_desc, rows);
+  const uint32_t tiles = pl.sort_map.n_tiles;
+  if (tiles + pl.seg.count > sc.sort_rows) return cudaErrorInvalidValue;
+  k_sort_init<D><<<pl.seg.count * sc.passes, 256, 0, s>>>(sc.ghist, sc.sort_desc, pl.seg,
+                                                          pl.sort_map, sc.passes, sc.sort_rows);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
   if (e != cudaSuccess) return e;
-  K* keys = static_cast<K*>(app.u_morton_keys);
-  K* alt = static_cast<K*>(app.u_morton_keys_alt);
-  K* tmp = static_cast<K*>(im->d_tmp_keys);
+  K* keys = static_cast<K*>(b.keys);
+  K* alt = static_cast<K*>(b.alt);
+  K* tmp = static_cast<K*>(b.tmp);
   const K* src = keys;
-  for (int p = 0; p < im->passes; ++p) {
-    K* dst = ((im->passes - 1 - p) % 2 == 0) ? alt : tmp;
-    kern<<<tiles, THREADS, C::kSmem, s>>>(
-        src, dst, n, p * D, im->d_sort_desc + size_t(p) * rows * C::RADIX,
-        im->d_tile_ctr + kCtrSortBase + p, im->d_status);
+  for (int p = 0; p < sc.passes; ++p) {
+    K* dst = ((sc.passes - 1 - p) % 2 == 0) ? alt : tmp;
+    if (tiles)
+      kern<<<tiles, THREADS, C::kSmem, s>>>(
+          src, dst, pl.seg, pl.sort_map, p * D,
+          sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
+          sc.tile_ctr + kCtrSortBase + p, sc.status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (marks) cudaEventRecord(marks[1 + p], s);
@@ -390,7 +394,7 @@ cudaError_t passes_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
   return cudaSuccess;
 }
 
-using PassFn = cudaError_t (*)(const rw_tree_app_data&, rw_tree_im_storage*, cudaStream_t,
+using PassFn = cudaError_t (*)(const Bufs&, const Scratch&, const Plan&, cudaStream_t,
                                cudaEvent_t*);
 
 struct SortVariant {
@@ -436,6 +440,11 @@ uint32_t sort_tile_for(int key_bits, int radix_bits) {
   return t;
 }
 
+uint32_t sort_variant_tile(int idx) {
+  if (idx < 0 || idx >= kNumVariants) return 0;
+  return uint32_t(kVariants[idx].threads * kVariants[idx].kpt);
+}
+
 int sort_variant_count() { return kNumVariants; }
 
 int sort_variant_info(int idx, int* key_bits, int* radix_bits, int* threads, int* kpt,
@@ -456,32 +465,22 @@ int default_sort_variant(int key_bits, int radix_bits) {
   return -1;
 }
 
-cudaError_t launch_morton(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          bool with_histogram, cudaStream_t s) {
-  if (app.key_bits == 32)
-    return im->radix_bits == 8 ? morton_t<uint32_t, 8>(app, im, with_histogram, s)
-                               : morton_t<uint32_t, 11>(app, im, with_histogram, s);
-  return im->radix_bits == 8 ? morton_t<uint64_t, 8>(app, im, with_histogram, s)
-                             : morton_t<uint64_t, 11>(app, im, with_histogram, s);
+cudaError_t launch_keys(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode,
+                        bool hist, cudaStream_t s) {
+  if (b.key_bits == 32)
+    return sc.radix_bits == 8 ? keys_t<uint32_t, 8>(b, sc, pl, encode, hist, s)
+                              : keys_t<uint32_t, 11>(b, sc, pl, encode, hist, s);
+  return sc.radix_bits == 8 ? keys_t<uint64_t, 8>(b, sc, pl, encode, hist, s)
+                            : keys_t<uint64_t, 11>(b, sc, pl, encode, hist, s);
 }
 
-cudaError_t launch_histogram(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                             cudaStream_t s) {
-  if (app.key_bits == 32)
-    return im->radix_bits == 8 ? histogram_t<uint32_t, 8>(app, im, s)
-                               : histogram_t<uint32_t, 11>(app, im, s);
-  return im->radix_bits == 8 ? histogram_t<uint64_t, 8>(app, im, s)
-                             : histogram_t<uint64_t, 11>(app, im, s);
-}
-
-cudaError_t launch_sort_passes(const rw_tree_app_data& app,
-                               rw_tree_im_storage* im, cudaStream_t s,
-                               cudaEvent_t* marks) {
-  const int v = im->sort_variant;
-  if (v < 0 || v >= kNumVariants || kVariants[v].key_bits != app.key_bits ||
-      kVariants[v].radix_bits != im->radix_bits)
+cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,
+                               cudaStream_t s, cudaEvent_t* marks) {
+  const int v = sc.sort_variant;
+  if (v < 0 || v >= kNumVariants || kVariants[v].key_bits != b.key_bits ||
+      kVariants[v].radix_bits != sc.radix_bits)
     return cudaErrorInvalidValue;
-  return kVariants[v].fn(app, im, s, marks);
+  return kVariants[v].fn(b, sc, pl, s, marks);
 }
 
 }  // namespace rwt

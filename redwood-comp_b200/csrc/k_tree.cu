@@ -34,30 +34,30 @@
 
 namespace rwt {
 
-__device__ __forceinline__ uint32_t count_of(Count c) {
-  return c.ptr ? *reinterpret_cast<const volatile uint32_t*>(c.ptr) : c.value;
-}
-
 // ---------------------------------------------------------------------------
 // stage 3: unique
 // ---------------------------------------------------------------------------
 
 template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
-    k_unique(const K* __restrict__ sorted, K* __restrict__ out, uint32_t n,
-             uint32_t* __restrict__ desc, uint32_t* __restrict__ tile_ctr,
-             DevStatus* __restrict__ st) {
+    k_unique(const K* __restrict__ sorted, K* __restrict__ out, SegTable seg, TileMap map,
+             uint32_t* __restrict__ n_unique, uint32_t* __restrict__ desc,
+             uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
   constexpr int KPT = kUniqueKpt, NW = kUniqueThreads / 32;
   __shared__ uint32_t s_warp[NW + 1];
   __shared__ uint32_t s_tile, s_excl;
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  const uint32_t n_tiles = (n + kUniqueTile - 1) / kUniqueTile;
   while (true) {
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    if (tile >= n_tiles) break;
-    const uint32_t wbase = tile * kUniqueTile + warp * 32u * KPT;
+    if (tile >= map.n_tiles) break;
+    uint32_t first;
+    const uint32_t c = tile_segment(seg, map, tile, &first);
+    const uint32_t sb = seg_begin(seg, c);
+    const uint32_t n = sb + seg_size(seg, c);  // end of the segment
+    const uint32_t last = map.toff ? map.toff[c + 1] - 1 : map.n_tiles - 1;
+    const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * KPT;
     K keys[KPT];
     uint32_t heads[KPT];
     K carry = K(0);
@@ -69,12 +69,12 @@ __global__ void __launch_bounds__(kUniqueThreads)
       K left = __shfl_up_sync(0xffffffffu, k, 1);
       if (lane == 0) {
         if (i == 0)
-          left = (wbase > 0 && wbase - 1 < n) ? sorted[wbase - 1] : K(~k);
+          left = (wbase > sb && wbase - 1 < n) ? sorted[wbase - 1] : K(~k);
         else
           left = carry;
       }
       carry = __shfl_sync(0xffffffffu, k, 31);
-      const bool head = idx < n && (idx == 0 || k != left);
+      const bool head = idx < n && (idx == sb || k != left);
       heads[i] = __ballot_sync(0xffffffffu, head);
       keys[i] = k;
       count += __popc(heads[i]);
@@ -82,25 +82,25 @@ __global__ void __launch_bounds__(kUniqueThreads)
     if (lane == 0) s_warp[warp] = count;
     __syncthreads();
     if (warp == 0) {
-      const uint32_t c = lane < NW ? s_warp[lane] : 0u;
-      const uint32_t inc = warp_inclusive_scan(c);
-      if (lane < NW) s_warp[lane] = inc - c;
+      const uint32_t cw = lane < NW ? s_warp[lane] : 0u;
+      const uint32_t inc = warp_inclusive_scan(cw);
+      if (lane < NW) s_warp[lane] = inc - cw;
       const uint32_t total = __shfl_sync(0xffffffffu, inc, NW - 1);
       uint32_t excl = 0;
-      if (tile == 0) {
-        if (lane == 0) st_relaxed(desc, kFlagInc | (total << 2));
+      if (tile == first) {
+        if (lane == 0) st_relaxed(desc + tile, kFlagInc | (total << 2));
       } else {
         if (lane == 0) st_relaxed(desc + tile, kFlagAgg | (total << 2));
-        excl = warp_lookback(desc, tile, st, kSiteUnique);
+        excl = warp_lookback(desc, tile, st, kSiteUnique, first);
         if (lane == 0) st_relaxed(desc + tile, kFlagInc | ((excl + total) << 2));
       }
       if (lane == 0) {
         s_excl = excl;
-        if (tile == n_tiles - 1) st->n_unique = excl + total;
+        if (tile == last) n_unique[c] = excl + total;
       }
     }
     __syncthreads();
-    uint32_t pos = s_excl + s_warp[warp];
+    uint32_t pos = sb + s_excl + s_warp[warp];
 #pragma unroll
     for (int i = 0; i < KPT; ++i) {
       const uint32_t dst = pos + __popc(heads[i] & lanemask_lt());
@@ -230,27 +230,36 @@ __device__ __forceinline__ int fused_edge_count(int i, int n, const KeyAt& key,
   return r.dnode / 3 - parent_prefix / 3;
 }
 
-// One CTA per tile of kTreeTile nodes; node base + q*kTreeThreads + tid for
-// q < kTreeNpt (striped, so every store instruction of a warp is contiguous).
+__device__ __forceinline__ void seg_error(int32_t* seg_err, uint32_t c, int32_t code) {
+  atomicCAS(reinterpret_cast<int*>(seg_err + c), 0, code);
+}
+
+// One CTA per tile of kTreeTile nodes (the tile map is sized by points, an
+// upper bound of the nodes); node base + q*kTreeThreads + tid for q <
+// kTreeNpt (striped, so every store instruction of a warp is contiguous).
 // With EDGES the kernel also writes edge_count (stages 4 and 5 in one pass);
 // tiles are independent, so no CTA ever waits for another.
 template <typename K, bool EDGES>
 __global__ void __launch_bounds__(kTreeThreads)
-    k_radix_tree(const K* __restrict__ codes, Count n_unique_c,
+    k_radix_tree(const K* __restrict__ codes_all, SegTable seg, TileMap map,
+                 const uint32_t* __restrict__ n_unique, int32_t* __restrict__ seg_err,
                  uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
                  uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
-                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
-                 DevStatus* __restrict__ st) {
+                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
   constexpr int NPT = kTreeNpt, HALO = kTreeHalo;
   constexpr int WIN = kTreeTile + 2 * HALO;
   __shared__ K s_win[WIN];
-  const uint32_t nu = count_of(n_unique_c);
-  if (nu < 3 || nu == RW_COUNT_UNSET) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) report_error(st, RW_ERR_DEGENERATE, kSiteTree);
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
+  const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
+  if (nu < 3 || nu == RW_COUNT_UNSET || nu > seg_size(seg, c)) {
+    if (blockIdx.x == first && threadIdx.x == 0) seg_error(seg_err, c, RW_ERR_DEGENERATE);
     return;
   }
+  const uint32_t sb = seg_begin(seg, c);
+  const K* codes = codes_all + sb;
   const int n = int(nu - 1);
-  const int base = int(blockIdx.x) * kTreeTile;
+  const int base = int(blockIdx.x - first) * kTreeTile;
   if (base >= n) return;
   const int wlo = base - HALO;
   for (int j = threadIdx.x; j < WIN; j += kTreeThreads) {
@@ -264,14 +273,19 @@ __global__ void __launch_bounds__(kTreeThreads)
     root_true_delta = delta(codes[0], codes[n]);
     root_prefix = delta(codes[0], codes[n - 1]);
   }
+  uint8_t* pn = prefix_n + sb;
+  uint8_t* l8 = hl + sb;
+  uint8_t* r8 = hr + sb;
+  int32_t* lcs = lc + sb;
+  int32_t* par = parents + sb;
 #pragma unroll 1
   for (int q = 0; q < NPT; ++q) {
     const int i = base + q * kTreeThreads + int(threadIdx.x);
     if (i >= n) break;
     const BrtNode r = brt_node<K>(i, n, key);
-    write_node<K>(i, n, key, r, prefix_n, hl, hr, lc, parents);
+    write_node<K>(i, n, key, r, pn, l8, r8, lcs, par);
     if (EDGES)
-      edge_count[i] =
+      edge_count[sb + i] =
           i > 0 ? fused_edge_count<K>(i, n, key, r, root_true_delta, root_prefix) : 0;
   }
 }
@@ -281,16 +295,23 @@ __global__ void __launch_bounds__(kTreeThreads)
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(256)
-    k_edge_count(const uint8_t* __restrict__ prefix_n,
-                 const int32_t* __restrict__ parents, int32_t* __restrict__ ec,
-                 Count n_unique_c) {
-  const int n = int(count_of(n_unique_c)) - 1;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const int p = parents[i];
+    k_edge_count(const uint8_t* __restrict__ prefix_n, const int32_t* __restrict__ parents,
+                 int32_t* __restrict__ ec, SegTable seg, TileMap map,
+                 const uint32_t* __restrict__ n_unique) {
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
+  const uint32_t nu = n_unique[c];
+  if (nu < 3 || nu == RW_COUNT_UNSET || nu > seg_size(seg, c)) return;
+  const int n = int(nu - 1);
+  const uint32_t sb = seg_begin(seg, c);
+  const int base = int(blockIdx.x - first) * kOctTile;
+  for (int q = 0; q < kOctNpt; ++q) {
+    const int i = base + q * kOctThreads + int(threadIdx.x);
+    if (i >= n) break;
+    const int p = parents[sb + i];
     // parents[] holds node indices in [0, n) after stage 4; anything else is a
     // caller error and reads node 0 instead of leaving the buffer
-    ec[i] = prefix_n[i] / 3 - prefix_n[uint32_t(p) < uint32_t(n) ? p : 0] / 3;
+    ec[sb + i] = prefix_n[sb + i] / 3 - prefix_n[sb + (uint32_t(p) < uint32_t(n) ? p : 0)] / 3;
   }
 }
 
@@ -299,24 +320,38 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kScanThreads)
-    k_edge_scan(const int32_t* __restrict__ ec, int32_t* __restrict__ off,
-                Count n_unique_c, uint32_t* __restrict__ desc,
+    k_edge_scan(const int32_t* __restrict__ ec_all, int32_t* __restrict__ off_all,
+                SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
+                uint32_t* __restrict__ n_octree, uint32_t* __restrict__ desc,
                 uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
   constexpr int KPT = kScanKpt, NW = kScanThreads / 32;
   __shared__ uint32_t s_warp[NW + 1];
   __shared__ uint32_t s_tile, s_excl;
-  const uint32_t n = count_of(n_unique_c) - 1;
-  const uint32_t n_tiles = (n + kScanTile - 1) / kScanTile;
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   while (true) {
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    if (tile >= n_tiles) break;
-    const uint32_t first = tile * kScanTile + tid * KPT;
+    if (tile >= map.n_tiles) break;
+    uint32_t firstt;
+    const uint32_t c = tile_segment(seg, map, tile, &firstt);
+    const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
+    const bool valid = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, c);
+    const uint32_t n = valid ? nu - 1 : 0;
+    const uint32_t n_tiles_c = (n + kScanTile - 1) / kScanTile;
+    const uint32_t j = tile - firstt;
+    if (j >= n_tiles_c) {  // beyond this segment's nodes (uniform across the CTA)
+      __syncthreads();
+      continue;
+    }
+    const uint32_t sb = seg_begin(seg, c);
+    const int32_t* ec = ec_all + sb;
+    int32_t* off = off_all + sb;
+    const uint32_t first = j * kScanTile + tid * KPT;
     int32_t v[KPT];
     uint32_t local = 0;
-    if (first + KPT <= n) {
+    const bool vec = first + KPT <= n && ((sb & 3u) == 0);
+    if (vec) {
 #pragma unroll
       for (int q = 0; q < KPT / 4; ++q) {
         const int4 x = reinterpret_cast<const int4*>(ec + first)[q];
@@ -332,21 +367,21 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t ex = block_exclusive_scan<kScanThreads>(local, s_warp, &total);
     if (warp == 0) {
       uint32_t excl = 0;
-      if (tile == 0) {
-        if (lane == 0) st_relaxed(desc, kFlagInc | (total << 2));
+      if (j == 0) {
+        if (lane == 0) st_relaxed(desc + tile, kFlagInc | (total << 2));
       } else {
         if (lane == 0) st_relaxed(desc + tile, kFlagAgg | (total << 2));
-        excl = warp_lookback(desc, tile, st, kSiteScan);
+        excl = warp_lookback(desc, tile, st, kSiteScan, firstt);
         if (lane == 0) st_relaxed(desc + tile, kFlagInc | ((excl + total) << 2));
       }
       if (lane == 0) {
         s_excl = excl;
-        if (tile == n_tiles - 1) st->n_octree_nodes = excl + total;
+        if (j == n_tiles_c - 1) n_octree[c] = excl + total;
       }
     }
     __syncthreads();
     uint32_t run = s_excl + ex;
-    if (first + KPT <= n) {
+    if (vec) {
 #pragma unroll
       for (int q = 0; q < KPT / 4; ++q) {
         int4 x;
@@ -377,8 +412,35 @@ struct OctOut {
   float* cell_size;
   int32_t* node_mask;
   int32_t* leaf_mask;
-  uint32_t capacity;
+  const uint32_t* oct_off;  // [segments + 1] row offsets; null with one segment
+  uint32_t capacity;        // rows with one segment
 };
+
+struct OctSeg {
+  uint32_t row0, cap, m;
+  int n;  // radix-tree nodes
+  bool ok;
+};
+
+// The segment's octree rows and counts; reports a too small octree.
+__device__ __forceinline__ OctSeg oct_segment(const SegTable& seg, const OctOut& o,
+                                              const uint32_t* n_unique,
+                                              const uint32_t* n_octree, int32_t* seg_err,
+                                              uint32_t c, bool report) {
+  OctSeg r{};
+  const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
+  r.ok = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, c);
+  if (!r.ok) return r;
+  r.n = int(nu - 1);
+  r.m = *reinterpret_cast<const volatile uint32_t*>(n_octree + c);
+  r.row0 = o.oct_off ? o.oct_off[c] : 0u;
+  r.cap = o.oct_off ? o.oct_off[c + 1] - o.oct_off[c] : o.capacity;
+  if (uint64_t(r.m) + 1 > r.cap) {
+    if (report) seg_error(seg_err, c, RW_ERR_CAPACITY);
+    r.ok = false;
+  }
+  return r;
+}
 
 // Rows [off[i], off[i] + cnt[i]) belong to radix-tree node i (i >= 1).  Row
 // off+k sits at level L - k (L = prefix_n[i] / 3); for k > 0 its one chain
@@ -386,48 +448,57 @@ struct OctOut {
 // thread writes the root initialisation when there is no octree node at all
 // (07_octree.cu:188-198) and clears the spare row m that a top link may name.
 template <typename K>
-__global__ void __launch_bounds__(256)
-    k_octree_rows(const K* __restrict__ codes, const uint8_t* __restrict__ prefix_n,
-                  const int32_t* __restrict__ ec, const int32_t* __restrict__ off,
-                  Count n_unique_c, Count n_oct_c, float min_coord, float range,
-                  OctOut o, DevStatus* __restrict__ st) {
+__global__ void __launch_bounds__(kOctThreads)
+    k_octree_rows(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
+                  const int32_t* __restrict__ ec_all, const int32_t* __restrict__ off_all,
+                  SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
+                  const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
+                  float min_coord, float range, OctOut o) {
   constexpr int B = KeyTraits<K>::kCodeBits;
-  const uint32_t nu = count_of(n_unique_c);
-  if (nu < 3 || nu == RW_COUNT_UNSET) return;
-  const int n = int(nu - 1);
-  const uint32_t m = count_of(n_oct_c);
-  if (uint64_t(m) + 1 > o.capacity) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) report_error(st, RW_ERR_CAPACITY, kSiteOctree);
-    return;
-  }
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
+  const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c,
+                                blockIdx.x == first && threadIdx.x == 0);
+  if (!os.ok) return;
+  const uint32_t sb = seg_begin(seg, c);
+  const K* codes = codes_all + sb;
+  const uint8_t* prefix_n = prefix_all + sb;
+  const int32_t* ec = ec_all + sb;
+  const int32_t* off = off_all + sb;
+  const int n = os.n;
+  const uint32_t m = os.m;
   const int root_level = prefix_n[0] / 3;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const int base = int(blockIdx.x - first) * kOctTile;
+  for (int q = 0; q < kOctNpt; ++q) {
+    const int i = base + q * kOctThreads + int(threadIdx.x);
+    if (i >= n) break;
     if (i == 0) {
-      int4* row = reinterpret_cast<int4*>(o.children + 8 * size_t(m));
+      const size_t rm = size_t(os.row0) + m;
+      int4* row = reinterpret_cast<int4*>(o.children + 8 * rm);
       row[0] = make_int4(0, 0, 0, 0);
       row[1] = make_int4(0, 0, 0, 0);
-      o.node_mask[m] = 0;
-      o.leaf_mask[m] = 0;
+      o.node_mask[rm] = 0;
+      o.leaf_mask[rm] = 0;
       if (m == 0) {
         const K pre = codes[0] >> (B - 3 * root_level);
-        o.corner[0] = decode<K>(K(pre << (B - 3 * root_level)), min_coord, range);
-        o.cell_size[0] = range;
+        o.corner[os.row0] = decode<K>(K(pre << (B - 3 * root_level)), min_coord, range);
+        o.cell_size[os.row0] = range;
       }
       continue;
     }
     const int cnt = ec[i];
     if (cnt <= 0) continue;
-    const int base = off[i];
+    const int rbase = off[i];
     const K code = codes[i];
     const int li = prefix_n[i] / 3;
     for (int k = 0; k < cnt; ++k) {
-      const int p = base + k;
+      const int p = rbase + k;
       if (uint32_t(p) >= m) break;  // rows of a consistent scan lie below m
+      const size_t rp = size_t(os.row0) + uint32_t(p);
       const int level = li - k;
       const K pre = code >> (B - 3 * level);
-      o.corner[p] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
-      o.cell_size[p] = __fdiv_rn(range, float(1 << (level - root_level)));
+      o.corner[rp] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
+      o.cell_size[rp] = __fdiv_rn(range, float(1 << (level - root_level)));
       int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       int32_t mask = 0;
       if (k > 0) {
@@ -435,11 +506,11 @@ __global__ void __launch_bounds__(256)
         child[slot] = p - 1;
         mask = 1 << slot;
       }
-      int4* row = reinterpret_cast<int4*>(o.children + 8 * size_t(p));
+      int4* row = reinterpret_cast<int4*>(o.children + 8 * rp);
       row[0] = make_int4(child[0], child[1], child[2], child[3]);
       row[1] = make_int4(child[4], child[5], child[6], child[7]);
-      o.node_mask[p] = mask;
-      o.leaf_mask[p] = 0;
+      o.node_mask[rp] = mask;
+      o.leaf_mask[rp] = 0;
     }
   }
 }
@@ -447,19 +518,29 @@ __global__ void __launch_bounds__(256)
 // Link of each chain's top row to the row of the nearest ancestor that owns
 // rows (func_octree.hpp:80-111; the walk gives up after 31 steps as there).
 template <typename K>
-__global__ void __launch_bounds__(256)
-    k_octree_links(const K* __restrict__ codes, const uint8_t* __restrict__ prefix_n,
-                   const int32_t* __restrict__ parents, const int32_t* __restrict__ ec,
-                   const int32_t* __restrict__ off, Count n_unique_c, Count n_oct_c,
-                   OctOut o) {
+__global__ void __launch_bounds__(kOctThreads)
+    k_octree_links(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
+                   const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
+                   const int32_t* __restrict__ off_all, SegTable seg, TileMap map,
+                   const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ n_octree,
+                   int32_t* __restrict__ seg_err, OctOut o) {
   constexpr int B = KeyTraits<K>::kCodeBits;
-  const uint32_t nu = count_of(n_unique_c);
-  if (nu < 3 || nu == RW_COUNT_UNSET) return;
-  const int n = int(nu - 1);
-  const uint32_t m = count_of(n_oct_c);
-  if (uint64_t(m) + 1 > o.capacity) return;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += stride) {
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
+  const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
+  if (!os.ok) return;
+  const uint32_t sb = seg_begin(seg, c);
+  const K* codes = codes_all + sb;
+  const uint8_t* prefix_n = prefix_all + sb;
+  const int32_t* parents = parents_all + sb;
+  const int32_t* ec = ec_all + sb;
+  const int32_t* off = off_all + sb;
+  const int n = os.n;
+  const int base = int(blockIdx.x - first) * kOctTile;
+  for (int q = 0; q < kOctNpt; ++q) {
+    const int i = base + q * kOctThreads + int(threadIdx.x);
+    if (i >= n) break;
+    if (i == 0) continue;
     const int cnt = ec[i];
     if (cnt <= 0) continue;
     int rp = parents[i];
@@ -474,9 +555,10 @@ __global__ void __launch_bounds__(256)
     const int oct_parent = off[rp];
     const int top = prefix_n[i] / 3 - cnt + 1;
     const int slot = int((codes[i] >> (B - 3 * top)) & K(7));
-    if (uint32_t(oct_parent) < o.capacity) {
-      atomicMax(o.children + 8 * size_t(oct_parent) + slot, off[i] + cnt - 1);
-      atomicOr(o.node_mask + oct_parent, 1 << slot);
+    if (uint32_t(oct_parent) < os.cap) {
+      const size_t r = size_t(os.row0) + uint32_t(oct_parent);
+      atomicMax(o.children + 8 * r + slot, off[i] + cnt - 1);
+      atomicOr(o.node_mask + r, 1 << slot);
     }
   }
 }
@@ -487,55 +569,56 @@ __global__ void __launch_bounds__(256)
 
 namespace {
 
-int persistent_blocks(rw_tree_im_storage* im, int per_sm) {
-  return im->num_sms * per_sm;
-}
+int persistent_blocks(const Scratch& sc, int per_sm) { return sc.num_sms * per_sm; }
 
 template <typename K>
-cudaError_t unique_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                     cudaStream_t s) {
-  const uint32_t tiles = div_up(app.n_input, kUniqueTile);
-  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(im, 8)));
+cudaError_t unique_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
+  const uint32_t tiles = pl.unique_map.n_tiles;
+  if (!tiles) return cudaSuccess;
+  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(sc, 8)));
   k_unique<K><<<blocks, kUniqueThreads, 0, s>>>(
-      static_cast<const K*>(app.u_morton_keys_alt), static_cast<K*>(app.u_morton_keys),
-      app.n_input, im->d_unique_desc, im->d_tile_ctr + kCtrUnique, im->d_status);
+      static_cast<const K*>(b.alt), static_cast<K*>(b.keys), pl.seg, pl.unique_map,
+      pl.n_unique, sc.unique_desc, sc.tile_ctr + kCtrUnique, sc.status);
   return cudaGetLastError();
 }
 
 template <typename K>
-cudaError_t tree_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                   Count nu, bool edges, cudaStream_t s) {
-  const uint32_t tiles = std::max(1u, div_up(app.n_input, kTreeTile));
-  const K* codes = static_cast<const K*>(app.u_morton_keys);
+cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
+                   cudaStream_t s) {
+  const uint32_t tiles = pl.tree_map.n_tiles;
+  if (!tiles) return cudaSuccess;
+  const K* codes = static_cast<const K*>(b.keys);
   if (edges)
     k_radix_tree<K, true><<<tiles, kTreeThreads, 0, s>>>(
-        codes, nu, app.brt_prefix_n, app.brt_has_leaf_left, app.brt_has_leaf_right,
-        app.brt_left_child, app.brt_parents, app.u_edge_count, im->d_status);
+        codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
+        b.parents, b.edge_count);
   else
     k_radix_tree<K, false><<<tiles, kTreeThreads, 0, s>>>(
-        codes, nu, app.brt_prefix_n, app.brt_has_leaf_left, app.brt_has_leaf_right,
-        app.brt_left_child, app.brt_parents, nullptr, im->d_status);
+        codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
+        b.parents, nullptr);
   return cudaGetLastError();
 }
 
 template <typename K>
-cudaError_t octree_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                     Count nu, Count nm, cudaStream_t s, cudaEvent_t* marks) {
-  OctOut o{app.oct_children, reinterpret_cast<float4*>(app.oct_corner),
-           app.oct_cell_size, app.oct_child_node_mask, app.oct_child_leaf_mask,
-           app.oct_capacity};
-  const K* codes = static_cast<const K*>(app.u_morton_keys);
-  const int blocks = std::max(1, std::min<int>(div_up(app.n_input, 256),
-                                               persistent_blocks(im, 8)));
-  k_octree_rows<K><<<blocks, 256, 0, s>>>(codes, app.brt_prefix_n, app.u_edge_count,
-                                          app.u_edge_offset, nu, nm, app.min_coord,
-                                          app.range, o, im->d_status);
+cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
+                     cudaEvent_t* marks) {
+  (void)sc;
+  OctOut o{b.children, b.corner, b.cell_size, b.node_mask, b.leaf_mask, pl.oct_off,
+           pl.oct_capacity};
+  const K* codes = static_cast<const K*>(b.keys);
+  const uint32_t tiles = pl.node_map.n_tiles;
+  if (tiles)
+    k_octree_rows<K><<<tiles, kOctThreads, 0, s>>>(
+        codes, b.prefix_n, b.edge_count, b.edge_offset, pl.seg, pl.node_map, pl.n_unique,
+        pl.n_octree, pl.seg_err, b.min_coord, b.range, o);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
-  k_octree_links<K><<<blocks, 256, 0, s>>>(codes, app.brt_prefix_n, app.brt_parents,
-                                           app.u_edge_count, app.u_edge_offset, nu,
-                                           nm, o);
+  if (tiles)
+    k_octree_links<K><<<tiles, kOctThreads, 0, s>>>(codes, b.prefix_n, b.parents,
+                                                    b.edge_count, b.edge_offset, pl.seg,
+                                                    pl.node_map, pl.n_unique, pl.n_octree,
+                                                    pl.seg_err, o);
   e = cudaGetLastError();
   if (e == cudaSuccess && marks) cudaEventRecord(marks[1], s);
   return e;
@@ -543,57 +626,72 @@ cudaError_t octree_t(const rw_tree_app_data& app, rw_tree_im_storage* im,
 
 }  // namespace
 
-cudaError_t launch_unique(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          cudaStream_t s) {
-  return app.key_bits == 32 ? unique_t<uint32_t>(app, im, s)
-                            : unique_t<uint64_t>(app, im, s);
+cudaError_t launch_unique(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
+  return b.key_bits == 32 ? unique_t<uint32_t>(b, sc, pl, s) : unique_t<uint64_t>(b, sc, pl, s);
 }
 
 cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
                               uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
                               int num_sms, cudaStream_t s) {
-  const uint32_t tiles = div_up(n, kUniqueTile);
-  const int blocks = std::max(1, std::min<int>(tiles, num_sms * 8));
-  if (key_bits == 32)
-    k_unique<uint32_t><<<blocks, kUniqueThreads, 0, s>>>(
-        static_cast<const uint32_t*>(sorted), static_cast<uint32_t*>(out), n, desc,
-        tile_ctr, status);
-  else
-    k_unique<uint64_t><<<blocks, kUniqueThreads, 0, s>>>(
-        static_cast<const uint64_t*>(sorted), static_cast<uint64_t*>(out), n, desc,
-        tile_ctr, status);
+  Bufs b;
+  b.key_bits = key_bits;
+  b.alt = const_cast<void*>(sorted);
+  b.keys = out;
+  Scratch sc;
+  sc.num_sms = num_sms;
+  sc.unique_desc = desc;
+  sc.tile_ctr = tile_ctr - kCtrUnique;
+  sc.status = status;
+  const Plan pl = single_plan(n, 0, status, 0);
+  return launch_unique(b, sc, pl, s);
+}
+
+cudaError_t launch_radix_tree(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
+                              cudaStream_t s) {
+  return b.key_bits == 32 ? tree_t<uint32_t>(b, sc, pl, edges, s)
+                          : tree_t<uint64_t>(b, sc, pl, edges, s);
+}
+
+cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
+                              cudaStream_t s) {
+  (void)sc;
+  if (!pl.node_map.n_tiles) return cudaSuccess;
+  k_edge_count<<<pl.node_map.n_tiles, kOctThreads, 0, s>>>(
+      b.prefix_n, b.parents, b.edge_count, pl.seg, pl.node_map, pl.n_unique);
   return cudaGetLastError();
 }
 
-cudaError_t launch_radix_tree(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                              Count nu, bool edges, cudaStream_t s) {
-  return app.key_bits == 32 ? tree_t<uint32_t>(app, im, nu, edges, s)
-                            : tree_t<uint64_t>(app, im, nu, edges, s);
-}
-
-cudaError_t launch_edge_count(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                              Count nu, cudaStream_t s) {
-  const int blocks = std::max(1, std::min<int>(div_up(app.n_input, 256),
-                                               persistent_blocks(im, 8)));
-  k_edge_count<<<blocks, 256, 0, s>>>(app.brt_prefix_n, app.brt_parents,
-                                      app.u_edge_count, nu);
+cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
+  const uint32_t tiles = pl.scan_map.n_tiles;
+  if (!tiles) return cudaSuccess;
+  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(sc, 8)));
+  k_edge_scan<<<blocks, kScanThreads, 0, s>>>(b.edge_count, b.edge_offset, pl.seg,
+                                              pl.scan_map, pl.n_unique, pl.n_octree,
+                                              sc.scan_desc, sc.tile_ctr + kCtrScan, sc.status);
   return cudaGetLastError();
 }
 
-cudaError_t launch_edge_scan(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                             Count nu, cudaStream_t s) {
-  const uint32_t tiles = div_up(app.n_input, kScanTile);
-  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(im, 8)));
-  k_edge_scan<<<blocks, kScanThreads, 0, s>>>(app.u_edge_count, app.u_edge_offset, nu,
-                                              im->d_scan_desc, im->d_tile_ctr + kCtrScan,
-                                              im->d_status);
-  return cudaGetLastError();
+cudaError_t launch_octree(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
+                          cudaEvent_t* marks) {
+  return b.key_bits == 32 ? octree_t<uint32_t>(b, sc, pl, s, marks)
+                          : octree_t<uint64_t>(b, sc, pl, s, marks);
 }
 
-cudaError_t launch_octree(const rw_tree_app_data& app, rw_tree_im_storage* im,
-                          Count nu, Count nm, cudaStream_t s, cudaEvent_t* marks) {
-  return app.key_bits == 32 ? octree_t<uint32_t>(app, im, nu, nm, s, marks)
-                            : octree_t<uint64_t>(app, im, nu, nm, s, marks);
+Plan single_plan(uint32_t n, uint32_t oct_capacity, DevStatus* status, uint32_t sort_tile) {
+  Plan pl;
+  pl.seg = SegTable{1u, n, nullptr};
+  pl.point_map = TileMap{div_up(n, kPointTile), nullptr};
+  pl.sort_map = TileMap{sort_tile ? div_up(n, sort_tile) : 0u, nullptr};
+  pl.unique_map = TileMap{div_up(n, kUniqueTile), nullptr};
+  pl.tree_map = TileMap{div_up(n, kTreeTile), nullptr};
+  pl.scan_map = TileMap{div_up(n, kScanTile), nullptr};
+  pl.node_map = TileMap{div_up(n, kOctTile), nullptr};
+  pl.n_unique = &status->n_unique;
+  pl.n_octree = &status->n_octree_nodes;
+  pl.seg_err = &status->err;
+  pl.oct_off = nullptr;
+  pl.oct_capacity = oct_capacity;
+  return pl;
 }
 
 }  // namespace rwt
