@@ -54,6 +54,8 @@ def parse_args():
                    help="onesweep variant index (default: the storage's default)")
     p.add_argument("--only-device", action="store_true",
                    help="time only the device-resident pipeline (for profiler runs)")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the batched and learned forms in the default line")
     return p.parse_args()
 
 
@@ -223,6 +225,93 @@ def run_reference(a, rank):
     return 0
 
 
+def batch_clouds(rw, n_clouds, seed, lo=1024, hi=262144):
+    """The batched configuration: sizes log-uniform in [lo, hi], each cloud
+    uniform or a Gaussian mixture with 8-64 components, chosen by seed."""
+    rng = np.random.default_rng(seed)
+    clouds = []
+    for c in range(n_clouds):
+        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        if rng.random() < 0.5:
+            clouds.append(rw.generate_points(n, rw.GEN_UNIFORM, seed * 7919 + c))
+        else:
+            clouds.append(rw.generate_points(n, rw.GEN_GAUSSIAN_MIXTURE, seed * 7919 + c,
+                                             n_components=int(rng.integers(8, 65))))
+    return clouds
+
+
+def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
+    """Batched pipeline (one graph launch per run) against the plain pipeline
+    run once per cloud on the same clouds, both bit-exact per cloud."""
+    import torch
+    from oracle import Oracle, ORC_OK
+    clouds = batch_clouds(rw, n_clouds, a.seed + 3)
+    total = int(sum(c.shape[0] for c in clouds))
+    ratio = 1.0  # octree rows per point: room for every cloud (0.6 overflows small ones)
+    batch = rw.Batch(clouds, a.key_bits, octree_ratio=ratio)
+    for _ in range(max(3, a.warmup)):
+        batch.run(graph=True)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(a.steps):
+        batch.enqueue(graph=True)
+    e1.record(s)
+    batch.finish()
+    batch_ms = e0.elapsed_time(e1) / a.steps
+    failed = int((batch.status != 0).sum())
+
+    # the plain pipeline once per cloud, launches back to back (no host sync
+    # between clouds), same capacity ratio
+    apps = [rw.AppData(c.shape[0], a.key_bits, points=c, octree_ratio=ratio) for c in clouds]
+    im_big = rw.ImStorage(max(c.shape[0] for c in clouds), a.key_bits)
+
+    def plain_once():
+        for app in apps:
+            rw.pipeline_enqueue(app, im_big)
+        rw.pipeline_finish(apps[-1], im_big)
+
+    plain_once()
+    torch.cuda.synchronize()
+    e0.record(s)
+    reps = 2
+    for _ in range(reps):
+        plain_once()
+    e1.record(s)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / reps
+
+    mism = 0
+    orc = Oracle()
+    rng = np.random.default_rng(5)
+    for c in sorted(rng.choice(n_clouds, size=min(verify_clouds, n_clouds), replace=False)):
+        want = orc.run(clouds[c], key_bits=a.key_bits, capacity=batch.capacity(c))
+        if want.status != ORC_OK:
+            mism += int(batch.status[c] == 0)
+            continue
+        got, w = batch.results(int(c)), want.trimmed()
+        mism += int(any(
+            np.ascontiguousarray(got[k]).tobytes() != np.ascontiguousarray(v).tobytes()
+            if isinstance(v, np.ndarray) else got[k] != v for k, v in w.items()))
+    info = {
+        "workload": f"batched: {n_clouds} clouds, sizes log-uniform in [1024, 262144] "
+                    f"(total {total:,} points), uniform or 8-64 component Gaussian mixture by "
+                    f"seed, {a.key_bits}-bit keys, octree rows {ratio} per point",
+        "value": total / (batch_ms / 1e3), "unit": "points/s", "ms_per_batch": batch_ms,
+        "plain_per_cloud_value": total / (plain_ms / 1e3), "plain_per_cloud_ms": plain_ms,
+        "speedup_vs_plain": plain_ms / batch_ms,
+        "clouds_failed": failed, "clouds_verified": min(verify_clouds, n_clouds),
+        "mismatches_vs_oracle": mism,
+        "tuning": batch.tuning and {"radix_bits": batch.tuning["radix_bits"],
+                                    "classes": [(c["max_points"], c["variant"]) for c in
+                                                batch.tuning["classes"]]},
+        "graph": True,
+    }
+    batch.close()
+    return info
+
+
 def cpu_baseline(rw, pts, a):
     from oracle import RefTree, ref_available
     if a.key_bits != 32 or not ref_available():
@@ -380,6 +469,12 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(rw, pts, a)
 
+    forms = None
+    if rank == 0 and not a.no_forms:
+        del app, im
+        torch.cuda.empty_cache()
+        forms = {"batched": measure_batch(rw, a)}
+
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -398,6 +493,7 @@ def main():
                               "frac": round(pipe_gbs / hbm, 4)},
         "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
         "clocks": clocks.summary(), "gpu_launches": (7 + passes) * a.steps,
+        "forms": forms,
     }
     print(json.dumps(line), flush=True)
     return 0

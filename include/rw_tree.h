@@ -256,7 +256,13 @@ uint32_t rw_tree_batch_octree_rows(const rw_tree_batch* batch);
 /* point_offsets and octree_offsets: [n_clouds + 1] each (either may be NULL). */
 int rw_tree_batch_offsets(const rw_tree_batch* batch, uint32_t* point_offsets,
                           uint32_t* octree_offsets);
+/* One onesweep variant for every cloud. */
 int rw_tree_batch_set_sort_variant(rw_tree_batch* batch, int32_t idx);
+/* Size classes of the sort (at most 4): a cloud of n points runs variant
+ * variants[k] for the first k with n <= max_points[k] (the last class takes
+ * every larger cloud).  The autotuner writes these tables. */
+int rw_tree_batch_set_classes(rw_tree_batch* batch, uint32_t n_classes,
+                              const uint32_t* max_points, const int32_t* variants);
 /* All stages for every cloud, asynchronous on `stream` (capturable). */
 int rw_tree_batch_enqueue(rw_tree_batch* batch, const rw_tree_batch_buffers* bufs,
                           rw_stream_t stream);

@@ -99,7 +99,7 @@ EXPORTS = (
     "rw_tree_unique_noalloc", "rw_tree_batch_create", "rw_tree_batch_destroy",
     "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
-    "rw_tree_batch_finish",
+    "rw_tree_batch_finish", "rw_tree_batch_set_classes",
 )
 
 
@@ -212,14 +212,17 @@ class AppData:
 
     def __init__(self, n_input: int, key_bits: int = 32,
                  points: Optional[np.ndarray] = None, device: str = "cuda",
-                 min_coord: float = 0.0, range_: float = 1024.0):
+                 min_coord: float = 0.0, range_: float = 1024.0,
+                 octree_ratio: Optional[float] = None):
         import torch
         if key_bits not in (32, 64):
             raise ValueError("key_bits must be 32 or 64")
         self.n_input = n = int(n_input)
         self.key_bits = key_bits
         self.min_coord, self.range = float(min_coord), float(range_)
-        self.oct_capacity = cap = octree_capacity(n)
+        # AppData's floor(0.6f * n) rows (app_data.hpp:13,28) unless a ratio is given
+        self.oct_capacity = cap = octree_capacity(n) if octree_ratio is None else \
+            int(np.float32(n) * np.float32(octree_ratio))
         kt = torch.int32 if key_bits == 32 else torch.int64
         dev = torch.device(device)
         e = lambda *shape, dtype: torch.zeros(*shape, dtype=dtype, device=dev)
@@ -245,6 +248,7 @@ class AppData:
         c = _AppDataC()
         lib().rw_tree_app_data_init(ctypes.byref(c), ctypes.c_uint32(n), ctypes.c_int32(key_bits))
         c.min_coord, c.range = self.min_coord, self.range
+        c.oct_capacity = cap
         for name, _ in _AppDataC._fields_:
             if hasattr(self, name) and name.startswith(("u_", "brt_", "oct_")) and name != "oct_capacity":
                 setattr(c, name, getattr(self, name).data_ptr())
@@ -373,8 +377,15 @@ class Batch:
     """
 
     def __init__(self, clouds, key_bits: int = 32, radix_bits: int = 0,
-                 octree_ratio: float = 0.6, device: str = "cuda"):
+                 octree_ratio: float = 0.6, device: str = "cuda", tuning="auto"):
+        """tuning: "auto" applies the autotuner's table for this key width when
+        one exists (tuning/b200_u{32,64}.json), None keeps the default
+        variant, a dict is used as the table."""
         import torch
+        from . import autotune
+        table = autotune.load_table(key_bits) if tuning == "auto" else tuning
+        if table and radix_bits == 0:
+            radix_bits = int(table["radix_bits"])
         sizes = np.array([c.shape[0] for c in clouds], np.uint32)
         self.n_clouds = len(clouds)
         self.key_bits = key_bits
@@ -418,6 +429,11 @@ class Batch:
         self.n_unique = np.zeros(self.n_clouds, np.uint32)
         self.n_octree_nodes = np.zeros(self.n_clouds, np.uint32)
         self.status = np.zeros(self.n_clouds, np.int32)
+        self.tuning = None
+        if table and int(table["radix_bits"]) == (radix_bits or 8) and \
+                int(table["key_bits"]) == key_bits:
+            self.set_classes(autotune.class_list(table))
+            self.tuning = table
 
     def capacity(self, c: int) -> int:
         return int(self.octree_offsets[c + 1] - self.octree_offsets[c])
@@ -429,6 +445,15 @@ class Batch:
 
     def set_sort_variant(self, idx: int) -> None:
         _check(lib().rw_tree_batch_set_sort_variant(self._h, idx), "batch_set_sort_variant")
+
+    def set_classes(self, classes) -> None:
+        """classes: [(max_points, variant_index), ...] ascending; the last
+        class takes every larger cloud."""
+        mx = np.array([c[0] for c in classes], np.uint32)
+        var = np.array([c[1] for c in classes], np.int32)
+        _check(lib().rw_tree_batch_set_classes(self._h, ctypes.c_uint32(len(classes)),
+                                               mx.ctypes.data_as(_vp), var.ctypes.data_as(_vp)),
+               "batch_set_classes")
 
     def enqueue(self, graph: bool = True, stream=None) -> None:
         fn = lib().rw_tree_batch_graph_launch if graph else lib().rw_tree_batch_enqueue

@@ -31,11 +31,20 @@ struct rw_tree_batch {
   // every kernel, each [n_clouds + 1]
   uint32_t* d_tables = nullptr;
   uint32_t *d_pt_off = nullptr, *d_oct_off = nullptr, *d_point_toff = nullptr,
-           *d_sort_toff = nullptr, *d_unique_toff = nullptr, *d_tree_toff = nullptr,
+           *d_unique_toff = nullptr, *d_tree_toff = nullptr,
            *d_scan_toff = nullptr, *d_node_toff = nullptr;
-  uint32_t point_tiles = 0, sort_tiles = 0, unique_tiles = 0, tree_tiles = 0,
+  uint32_t point_tiles = 0, unique_tiles = 0, tree_tiles = 0,
            scan_tiles = 0, node_tiles = 0;
-  uint32_t sort_rows = 0;  // rows per pass, sized for the smallest sort tile
+  uint32_t sort_rows = 0;  // rows per pass (stride), room for kMaxSortClasses classes
+
+  // size classes of the sort: clouds with n_c <= class_max[k] (first match)
+  // run variant class_variant[k]; each class has its own tile map and rows
+  uint32_t n_classes = 1;
+  uint32_t class_max[rwt::kMaxSortClasses] = {0xffffffffu};
+  int class_variant[rwt::kMaxSortClasses] = {0};
+  uint32_t class_tiles[rwt::kMaxSortClasses] = {0};
+  uint32_t class_base[rwt::kMaxSortClasses] = {0};  // first descriptor row
+  uint32_t* d_class_toff = nullptr;                  // [kMaxSortClasses][n_clouds + 1]
 
   void* d_tmp_keys = nullptr;
   void* d_zero = nullptr;
@@ -77,12 +86,34 @@ std::vector<uint32_t> tile_offsets(const std::vector<uint32_t>& pt_off, uint32_t
   return t;
 }
 
-int upload_sort_map(rw_tree_batch* b) {
-  const uint32_t tile = rwt::sort_variant_tile(b->sort_variant);
-  const auto t = tile_offsets(b->h_pt_off, tile);
-  b->sort_tiles = t.back();
-  if (b->sort_tiles + b->n_clouds > b->sort_rows) return RW_ERR_ARG;
-  RWB_CUDA(cudaMemcpy(b->d_sort_toff, t.data(), 4 * t.size(), cudaMemcpyHostToDevice));
+// Tile maps and descriptor rows of the sort's size classes.
+int upload_classes(rw_tree_batch* b) {
+  const size_t tab = size_t(b->n_clouds) + 1;
+  std::vector<uint32_t> all;
+  all.reserve(rwt::kMaxSortClasses * tab);
+  uint32_t base = 0;
+  for (uint32_t k = 0; k < rwt::kMaxSortClasses; ++k) {
+    std::vector<uint32_t> t(tab, 0);
+    if (k < b->n_classes) {
+      const uint32_t tile = rwt::sort_variant_tile(b->class_variant[k]);
+      for (uint32_t c = 0; c < b->n_clouds; ++c) {
+        const uint32_t n = b->h_pt_off[c + 1] - b->h_pt_off[c];
+        uint32_t cls = b->n_classes - 1;
+        for (uint32_t j = 0; j < b->n_classes; ++j)
+          if (n <= b->class_max[j]) {
+            cls = j;
+            break;
+          }
+        t[c + 1] = t[c] + (cls == k ? rwt::div_up(n, tile) : 0u);
+      }
+      b->class_tiles[k] = t.back();
+      b->class_base[k] = base;
+      base += t.back() + b->n_clouds;
+    }
+    all.insert(all.end(), t.begin(), t.end());
+  }
+  if (base > b->sort_rows) return RW_ERR_ARG;
+  RWB_CUDA(cudaMemcpy(b->d_class_toff, all.data(), 4 * all.size(), cudaMemcpyHostToDevice));
   return RW_OK;
 }
 
@@ -130,7 +161,7 @@ rwt::Plan plan_of(const rw_tree_batch* b) {
   rwt::Plan pl;
   pl.seg = rwt::SegTable{b->n_clouds, b->n_total, b->d_pt_off};
   pl.point_map = rwt::TileMap{b->point_tiles, b->d_point_toff};
-  pl.sort_map = rwt::TileMap{b->sort_tiles, b->d_sort_toff};
+  pl.sort_map = rwt::TileMap{b->class_tiles[0], b->d_class_toff};
   pl.unique_map = rwt::TileMap{b->unique_tiles, b->d_unique_toff};
   pl.tree_map = rwt::TileMap{b->tree_tiles, b->d_tree_toff};
   pl.scan_map = rwt::TileMap{b->scan_tiles, b->d_scan_toff};
@@ -204,6 +235,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   b->radix_bits = radix_bits ? radix_bits : 8;
   b->passes = (code_bits(key_bits) + b->radix_bits - 1) / b->radix_bits;
   b->sort_variant = rwt::default_sort_variant(key_bits, b->radix_bits);
+  b->class_variant[0] = b->sort_variant;
 
   b->h_pt_off.assign(n_clouds + 1, 0);
   b->h_oct_off.assign(n_clouds + 1, 0);
@@ -227,7 +259,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   b->tree_tiles = tree_t.back();
   b->scan_tiles = scan_t.back();
   b->node_tiles = node_t.back();
-  b->sort_rows = min_sort_t.back() + n_clouds;
+  b->sort_rows = min_sort_t.back() + rwt::kMaxSortClasses * n_clouds;
 
   const size_t tab = size_t(n_clouds) + 1;
   const size_t radix = size_t(1) << b->radix_bits;
@@ -242,7 +274,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   b->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b + 3 * per_b;
 
   const size_t ks = key_bits == 32 ? 4 : 8;
-  cudaError_t e = cudaMalloc(&b->d_tables, 8 * tab * 4);
+  cudaError_t e = cudaMalloc(&b->d_tables, (8 + rwt::kMaxSortClasses) * tab * 4);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tmp_keys, ks * total);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_zero, b->zero_bytes);
   if (e == cudaSuccess) e = cudaMallocHost(&b->h_results, (3 * size_t(n_clouds) + 4) * 4);
@@ -254,11 +286,12 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   b->d_pt_off = t;
   b->d_oct_off = t + tab;
   b->d_point_toff = t + 2 * tab;
-  b->d_sort_toff = t + 3 * tab;
+  // t + 3 * tab: the smallest-tile sort map (sizing only)
   b->d_unique_toff = t + 4 * tab;
   b->d_tree_toff = t + 5 * tab;
   b->d_scan_toff = t + 6 * tab;
   b->d_node_toff = t + 7 * tab;
+  b->d_class_toff = t + 8 * tab;
   char* z = static_cast<char*>(b->d_zero);
   size_t o = 0;
   b->d_ghist = reinterpret_cast<uint32_t*>(z + o); o += ghist_b;
@@ -278,7 +311,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   for (const auto* v : parts) all.insert(all.end(), v->begin(), v->end());
   e = cudaMemcpy(b->d_tables, all.data(), 4 * all.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(b->d_zero, 0, b->zero_bytes);
-  if (e != cudaSuccess || upload_sort_map(b) != RW_OK) {
+  if (e != cudaSuccess || upload_classes(b) != RW_OK) {
     rw_tree_batch_destroy(b);
     return RW_ERR_CUDA;
   }
@@ -311,17 +344,42 @@ int rw_tree_batch_offsets(const rw_tree_batch* b, uint32_t* point_offsets,
 }
 
 int rw_tree_batch_set_sort_variant(rw_tree_batch* b, int32_t idx) {
-  int kb, rb, th, kpt, rk;
-  if (!b || rwt::sort_variant_info(idx, &kb, &rb, &th, &kpt, &rk) != 0) return RW_ERR_ARG;
-  if (kb != b->key_bits || rb != b->radix_bits) return RW_ERR_ARG;
-  const int old = b->sort_variant;
-  b->sort_variant = idx;
-  if (int rc = upload_sort_map(b)) {
-    b->sort_variant = old;
-    upload_sort_map(b);
+  const uint32_t all = 0xffffffffu;
+  return rw_tree_batch_set_classes(b, 1, &all, &idx);
+}
+
+int rw_tree_batch_set_classes(rw_tree_batch* b, uint32_t n_classes, const uint32_t* max_points,
+                              const int32_t* variants) {
+  if (!b || n_classes < 1 || n_classes > uint32_t(rwt::kMaxSortClasses) || !max_points ||
+      !variants)
+    return RW_ERR_ARG;
+  for (uint32_t k = 0; k < n_classes; ++k) {
+    int kb, rb, th, kpt, rk;
+    if (rwt::sort_variant_info(variants[k], &kb, &rb, &th, &kpt, &rk) != 0) return RW_ERR_ARG;
+    if (kb != b->key_bits || rb != b->radix_bits) return RW_ERR_ARG;
+    if (k > 0 && max_points[k] <= max_points[k - 1]) return RW_ERR_ARG;
+  }
+  // keep the current classes to restore them if the new ones do not fit
+  const uint32_t old_n = b->n_classes;
+  uint32_t old_max[rwt::kMaxSortClasses];
+  int old_var[rwt::kMaxSortClasses];
+  std::memcpy(old_max, b->class_max, sizeof old_max);
+  std::memcpy(old_var, b->class_variant, sizeof old_var);
+  b->n_classes = n_classes;
+  for (uint32_t k = 0; k < n_classes; ++k) {
+    b->class_max[k] = max_points[k];
+    b->class_variant[k] = variants[k];
+  }
+  b->class_max[n_classes - 1] = 0xffffffffu;  // the last class takes the rest
+  if (int rc = upload_classes(b)) {
+    b->n_classes = old_n;
+    std::memcpy(b->class_max, old_max, sizeof old_max);
+    std::memcpy(b->class_variant, old_var, sizeof old_var);
+    upload_classes(b);
     return rc;
   }
-  release_graph(b);  // the captured graph used the previous variant
+  b->sort_variant = variants[0];
+  release_graph(b);  // the captured graph used the previous classes
   return RW_OK;
 }
 
@@ -334,7 +392,17 @@ int rw_tree_batch_enqueue(rw_tree_batch* b, const rw_tree_batch_buffers* u, rw_s
   const auto pl = plan_of(b);
   RWB_CUDA(cudaMemsetAsync(b->d_zero, 0, b->zero_bytes, s));
   RWB_CUDA(rwt::launch_keys(x, sc, pl, true, true, s));
-  RWB_CUDA(rwt::launch_sort_passes(x, sc, pl, s));
+  const size_t radix = size_t(1) << b->radix_bits;
+  for (uint32_t k = 0; k < b->n_classes; ++k) {
+    if (!b->class_tiles[k]) continue;
+    rwt::Scratch sk = sc;
+    sk.sort_variant = b->class_variant[k];
+    sk.sort_desc = b->d_sort_desc + size_t(b->class_base[k]) * radix;
+    sk.tile_ctr = b->d_tile_ctr + k * rwt::kCtrSortClassStride;
+    rwt::Plan pk = pl;
+    pk.sort_map = rwt::TileMap{b->class_tiles[k], b->d_class_toff + k * (size_t(b->n_clouds) + 1)};
+    RWB_CUDA(rwt::launch_sort_passes(x, sk, pk, s));
+  }
   RWB_CUDA(rwt::launch_unique(x, sc, pl, s));
   RWB_CUDA(rwt::launch_radix_tree(x, sc, pl, true, s));
   RWB_CUDA(rwt::launch_edge_scan(x, sc, pl, s));

@@ -44,7 +44,7 @@ struct rw_tree_im_storage {
 namespace rwt {
 
 enum : int { kCtrUnique = 0, kCtrScan = 1, kCtrTree = 2, kCtrSortBase = 4,
-             kCounters = 32 };
+             kCtrSortClassStride = 8, kMaxSortClasses = 4, kCounters = 64 };
 
 // Tile sizes of the kernels (points or nodes per tile).
 constexpr uint32_t kPointTile = 4096;  // Morton / histogram

@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(256)
   __shared__ uint32_t s_warp[9];
   const uint32_t c = blockIdx.x / passes;
   const int pass = int(blockIdx.x % passes);
+  if (map.toff && map.toff[c + 1] == map.toff[c]) return;  // no tile in this map
   const uint32_t* h = ghist + (size_t(c) * passes + pass) * RADIX;
   const uint32_t init_row = (map.toff ? map.toff[c] : 0u) + c;
   uint32_t* row0 = desc + (size_t(pass) * rows_per_pass + init_row) * RADIX;

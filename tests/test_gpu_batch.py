@@ -90,3 +90,13 @@ def test_batch_eleven_bit_digits(rw, oracle):
     batch = rw.Batch(clouds, 32, radix_bits=11)
     batch.run(graph=True)
     check_batch(rw, oracle, batch, clouds, 32)
+
+
+def test_batch_size_classes(rw, oracle):
+    """Three size classes, each with its own onesweep variant, in one batch."""
+    clouds = make_clouds(rw, 40, 500, 120000, 21)
+    v32 = [v["index"] for v in rw.sort_variants() if v["key_bits"] == 32 and v["radix_bits"] == 8]
+    batch = rw.Batch(clouds, 32, octree_ratio=1.5, tuning=None)
+    batch.set_classes([(4000, v32[2]), (30000, v32[1]), (1 << 30, v32[0])])
+    batch.run(graph=True)
+    assert check_batch(rw, oracle, batch, clouds, 32)["ok"] == len(clouds)
