@@ -277,6 +277,65 @@ int rw_tree_batch_graph_launch(rw_tree_batch* batch, const rw_tree_batch_buffers
 int rw_tree_batch_finish(rw_tree_batch* batch, rw_stream_t stream, uint32_t* n_unique,
                          uint32_t* n_octree_nodes, int32_t* status);
 
+/* Stage 2 alone, asynchronous on `stream` (no synchronisation, capturable):
+ * sorts app->u_morton_keys[0, n) into app->u_morton_keys_alt with the onesweep
+ * sort.  Only the two key buffers of `app` are used. */
+int rw_tree_sort_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im, rw_stream_t stream);
+
+/* ---- learned-CDF bucketed sort (32-bit keys) -------------------------------
+ * No reference counterpart.  A 64K-key stratified sample is sorted; 4,095
+ * bucket boundaries are placed inside windows of 16 sorted sample keys, by the
+ * boundary MLP (16 -> 64 -> 64 -> 1, BF16 weights, FP32 accumulate) or at the
+ * windows' middle keys (plain sample quantiles, the method without the
+ * network); keys are scattered into the 4,096 buckets in one pass and each
+ * bucket is sorted exactly.  A bucket larger than 2^21 keys sends the whole
+ * input to the onesweep sort.  The output is the sorted input either way. */
+typedef struct rw_tree_learned rw_tree_learned;
+#define RW_LEARNED_MLP 0
+#define RW_LEARNED_SAMPLE_QUANTILES 1
+#define RW_LEARNED_MLP_PARAMS 5313 /* 16*64 + 64 + 64*64 + 64 + 64 + 1 */
+
+typedef struct rw_tree_learned_stats {
+  uint32_t max_bucket;  /* keys in the fullest bucket */
+  uint32_t big_buckets; /* buckets sorted by the chunked single-CTA path */
+  uint32_t fell_back;   /* 1 when the onesweep sort ran instead */
+  uint32_t reserved;
+} rw_tree_learned_stats;
+
+/* Scratch for inputs of up to n_max (>= 65536) keys on the current device. */
+int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out);
+int rw_tree_learned_destroy(rw_tree_learned* learned);
+/* FP32 master parameters (RW_LEARNED_MLP_PARAMS floats, layout W1[64][16],
+ * b1[64], W2[64][64], b2[64], W3[64], b3); used rounded to BF16. */
+int rw_tree_learned_set_params(rw_tree_learned* learned, const float* params, int32_t count);
+/* Sorts d_keys[0, n) into d_sorted.  `fallback_im` (storage for n keys) runs
+ * the onesweep sort when needed; stats may be NULL.  Synchronises once (the
+ * bucket plan decides the path). */
+int rw_tree_learned_sort(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t* d_sorted,
+                         uint32_t n, int32_t mode, rw_tree_im_storage* fallback_im,
+                         rw_stream_t stream, rw_tree_learned_stats* stats);
+/* The MLP inputs of the 4,095 boundaries for d_keys (training data), the
+ * window bases and spans, and the plain sample-quantile boundaries (host
+ * arrays, any may be NULL: [4095*16], [4095], [4095], [4095]). */
+int rw_tree_learned_features(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
+                             float* features, uint32_t* window_lo, uint32_t* window_span,
+                             uint32_t* sample_quantiles, rw_stream_t stream);
+/* Keys per bucket (host [4096]) under `mode`'s boundaries. */
+int rw_tree_learned_bucket_counts(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
+                                  int32_t mode, uint32_t* counts, rw_stream_t stream);
+
+/* Training kernels of the boundary MLP (device arrays).  x: [rows][16],
+ * t: [rows]; mean squared error over `batch` examples (rows of this call may
+ * be a part of the batch).  grad and loss_sum are accumulated into. */
+int rw_tree_mlp_param_count(void);
+int rw_tree_mlp_grad(const float* params, const float* x, const float* t, uint32_t rows,
+                     uint32_t batch, float* grad, float* loss_sum, rw_stream_t stream);
+/* Adam step (bias-corrected) on the FP32 master parameters; step >= 1. */
+int rw_tree_mlp_adam(float* params, const float* grad, float* m, float* v, float lr,
+                     float beta1, float beta2, float eps, int32_t step, rw_stream_t stream);
+int rw_tree_mlp_forward(const float* params, const float* x, uint32_t rows, float* y,
+                        rw_stream_t stream);
+
 /* Stage 3 for callers that cannot allocate GPU memory (a host whose device
  * memory is all reserved by its own pool, a real-time loop that must not take
  * the driver's allocation locks, a plugin given only pointers and a stream).

@@ -99,7 +99,10 @@ EXPORTS = (
     "rw_tree_unique_noalloc", "rw_tree_batch_create", "rw_tree_batch_destroy",
     "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
-    "rw_tree_batch_finish", "rw_tree_batch_set_classes",
+    "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
+    "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
+    "rw_tree_learned_sort", "rw_tree_learned_features", "rw_tree_learned_bucket_counts",
+    "rw_tree_mlp_param_count", "rw_tree_mlp_grad", "rw_tree_mlp_adam", "rw_tree_mlp_forward",
 )
 
 
@@ -506,3 +509,118 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# learned-CDF bucketed sort and its boundary MLP
+# ---------------------------------------------------------------------------
+
+LEARNED_MLP, LEARNED_SAMPLE_QUANTILES = 0, 1
+MLP_PARAMS = 5313
+
+
+class _LearnedStatsC(ctypes.Structure):
+    _fields_ = [("max_bucket", ctypes.c_uint32), ("big_buckets", ctypes.c_uint32),
+                ("fell_back", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def _dptr(t) -> _vp:
+    return _vp(t.data_ptr())
+
+
+class Learned:
+    """Scratch and boundary-MLP parameters of the learned-CDF sort.
+
+    params: "auto" loads the trained table (tuning/cdf_mlp_b200.json) when
+    present, None leaves the network unset (sample quantiles only), or a
+    float32 array of MLP_PARAMS values."""
+
+    def __init__(self, n_max: int, params="auto"):
+        self._h = _vp()
+        _check(lib().rw_tree_learned_create(ctypes.c_uint32(n_max), ctypes.byref(self._h)),
+               "Learned")
+        self.n_max = n_max
+        self.params = None
+        if isinstance(params, str) and params == "auto":
+            from . import learned as _learned
+            params = _learned.load_params()
+        if params is not None:
+            self.set_params(params)
+
+    def set_params(self, params) -> None:
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        _check(lib().rw_tree_learned_set_params(self._h, p.ctypes.data_as(_vp),
+                                                ctypes.c_int32(p.size)), "learned_set_params")
+        self.params = p
+
+    def sort(self, keys, out=None, mode: int = LEARNED_MLP, fallback_im=None, stream=None):
+        """Sorts a device int32 tensor of 32-bit keys; returns (sorted, stats)."""
+        import torch
+        n = keys.numel()
+        out = torch.empty_like(keys) if out is None else out
+        st = _LearnedStatsC()
+        im = fallback_im.handle if fallback_im is not None else None
+        _check(lib().rw_tree_learned_sort(self._h, _dptr(keys), _dptr(out), ctypes.c_uint32(n),
+                                          ctypes.c_int32(mode), im, _stream_handle(stream),
+                                          ctypes.byref(st)), "learned_sort")
+        return out, {"max_bucket": st.max_bucket, "big_buckets": st.big_buckets,
+                     "fell_back": st.fell_back}
+
+    def features(self, keys, stream=None):
+        """MLP inputs [4095,16], window bases and spans, sample quantiles."""
+        n = keys.numel()
+        f = np.zeros((4095, 16), np.float32)
+        lo = np.zeros(4095, np.uint32)
+        span = np.zeros(4095, np.uint32)
+        sq = np.zeros(4095, np.uint32)
+        _check(lib().rw_tree_learned_features(self._h, _dptr(keys), ctypes.c_uint32(n),
+                                              f.ctypes.data_as(_vp), lo.ctypes.data_as(_vp),
+                                              span.ctypes.data_as(_vp), sq.ctypes.data_as(_vp),
+                                              _stream_handle(stream)), "learned_features")
+        return f, lo, span, sq
+
+    def bucket_counts(self, keys, mode: int = LEARNED_MLP, stream=None) -> np.ndarray:
+        c = np.zeros(4096, np.uint32)
+        _check(lib().rw_tree_learned_bucket_counts(self._h, _dptr(keys), ctypes.c_uint32(keys.numel()),
+                                                   ctypes.c_int32(mode), c.ctypes.data_as(_vp),
+                                                   _stream_handle(stream)), "bucket_counts")
+        return c
+
+    def close(self) -> None:
+        if self._h:
+            lib().rw_tree_learned_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_grad(params, x, t, batch: int, grad=None, loss=None, stream=None):
+    """Accumulates d(MSE over `batch`)/d(params) of rows (x, t) into grad
+    (device float32 tensors); returns (grad, loss_sum)."""
+    import torch
+    grad = torch.zeros_like(params) if grad is None else grad
+    loss = torch.zeros(1, dtype=torch.float32, device=params.device) if loss is None else loss
+    _check(lib().rw_tree_mlp_grad(_dptr(params), _dptr(x), _dptr(t), ctypes.c_uint32(t.numel()),
+                                  ctypes.c_uint32(batch), _dptr(grad), _dptr(loss),
+                                  _stream_handle(stream)), "mlp_grad")
+    return grad, loss
+
+
+def mlp_adam(params, grad, m, v, lr: float, step: int, beta1=0.9, beta2=0.999, eps=1e-8,
+             stream=None) -> None:
+    _check(lib().rw_tree_mlp_adam(_dptr(params), _dptr(grad), _dptr(m), _dptr(v),
+                                  ctypes.c_float(lr), ctypes.c_float(beta1), ctypes.c_float(beta2),
+                                  ctypes.c_float(eps), ctypes.c_int32(step),
+                                  _stream_handle(stream)), "mlp_adam")
+
+
+def mlp_forward(params, x, stream=None):
+    import torch
+    y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
+    _check(lib().rw_tree_mlp_forward(_dptr(params), _dptr(x), ctypes.c_uint32(x.shape[0]),
+                                     _dptr(y), _stream_handle(stream)), "mlp_forward")
+    return y

@@ -299,6 +299,18 @@ int rw_tree_run_stage2(rw_tree_app_data* app, rw_tree_im_storage* im,
   return sync_status(im, s);
 }
 
+int rw_tree_sort_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im, rw_stream_t stream) {
+  if (int rc = check(app, im, kKeys | kAlt)) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (int rc = clear_all(im, s)) return rc;
+  const auto b = bufs_of(*app, im);
+  const auto sc = scratch_of(im);
+  const auto pl = plan_of(*app, im);
+  RW_CUDA(rwt::launch_keys(b, sc, pl, false, true, s));
+  RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s));
+  return RW_OK;
+}
+
 // ---- stage 3: unique (cu_dispatcher.cu:597-627) -------------------------------
 int rw_tree_run_stage3(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {

