@@ -304,8 +304,10 @@ def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
         "clouds_failed": failed, "clouds_verified": min(verify_clouds, n_clouds),
         "mismatches_vs_oracle": mism,
         "tuning": batch.tuning and {"radix_bits": batch.tuning["radix_bits"],
-                                    "classes": [(c["max_points"], c["variant"]) for c in
-                                                batch.tuning["classes"]]},
+                                    "classes": [(c["max_points"],
+                                                 f'{c["threads"]}x{c["keys_per_thread"]} '
+                                                 f'{("ballot", "match_any", "atomic_or")[c["rank"]]}')
+                                                for c in batch.tuning["classes"]]},
         "graph": True,
     }
     batch.close()

@@ -281,19 +281,30 @@ int rw_tree_batch_finish(rw_tree_batch* batch, rw_stream_t stream, uint32_t* n_u
  * sorts app->u_morton_keys[0, n) into app->u_morton_keys_alt with the onesweep
  * sort.  Only the two key buffers of `app` are used. */
 int rw_tree_sort_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im, rw_stream_t stream);
+/* The same sort `reps` times with CUDA events between its kernels; mean
+ * device milliseconds of the digit histogram, the pass set-up and each pass
+ * (2 + passes entries, in that order) into kernel_ms.  Synchronous. */
+int rw_tree_sort_profile(rw_tree_app_data* app, rw_tree_im_storage* im, rw_stream_t stream,
+                         int32_t reps, float* kernel_ms, int32_t max_kernels,
+                         int32_t* n_kernels);
 
 /* ---- learned-CDF bucketed sort (32-bit keys) -------------------------------
- * No reference counterpart.  A 64K-key stratified sample is sorted; 4,095
- * bucket boundaries are placed inside windows of 16 sorted sample keys, by the
- * boundary MLP (16 -> 64 -> 64 -> 1, BF16 weights, FP32 accumulate) or at the
- * windows' middle keys (plain sample quantiles, the method without the
- * network); keys are scattered into the 4,096 buckets in one pass and each
- * bucket is sorted exactly.  A bucket larger than 2^21 keys sends the whole
- * input to the onesweep sort.  The output is the sorted input either way. */
+ * No reference counterpart.  A 64K-key stratified sample is sorted and 4,095
+ * bucket boundaries are placed, one per 16 sample ranks: at the sample key of
+ * rank 16(j+1) (plain sample quantiles, the method without the network), or
+ * by the boundary MLP (16 -> 64 -> 64 -> 1, BF16 weights, FP32 accumulate),
+ * which reads a context of 16 groups of `group` sorted sample keys around that
+ * rank (input i = mean position of group i inside the context's key range)
+ * and returns the boundary's position in that range; it is clamped into the
+ * boundary's own 16 sample ranks, so boundaries never decrease.  Keys are
+ * scattered into the 4,096 buckets in one pass and each bucket is sorted
+ * exactly.  A bucket larger than 2^21 keys sends the whole input to the
+ * onesweep sort.  The output is the sorted input either way. */
 typedef struct rw_tree_learned rw_tree_learned;
 #define RW_LEARNED_MLP 0
 #define RW_LEARNED_SAMPLE_QUANTILES 1
 #define RW_LEARNED_MLP_PARAMS 5313 /* 16*64 + 64 + 64*64 + 64 + 64 + 1 */
+#define RW_LEARNED_MAX_GROUP 16    /* group: a power of two, 1..16 */
 
 typedef struct rw_tree_learned_stats {
   uint32_t max_bucket;  /* keys in the fullest bucket */
@@ -306,20 +317,24 @@ typedef struct rw_tree_learned_stats {
 int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out);
 int rw_tree_learned_destroy(rw_tree_learned* learned);
 /* FP32 master parameters (RW_LEARNED_MLP_PARAMS floats, layout W1[64][16],
- * b1[64], W2[64][64], b2[64], W3[64], b3); used rounded to BF16. */
-int rw_tree_learned_set_params(rw_tree_learned* learned, const float* params, int32_t count);
+ * b1[64], W2[64][64], b2[64], W3[64], b3; used rounded to BF16) and the
+ * context group size they were trained with. */
+int rw_tree_learned_set_params(rw_tree_learned* learned, const float* params, int32_t count,
+                               int32_t group);
+/* Context group size alone (for rw_tree_learned_features); default 4. */
+int rw_tree_learned_set_group(rw_tree_learned* learned, int32_t group);
 /* Sorts d_keys[0, n) into d_sorted.  `fallback_im` (storage for n keys) runs
  * the onesweep sort when needed; stats may be NULL.  Synchronises once (the
  * bucket plan decides the path). */
 int rw_tree_learned_sort(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t* d_sorted,
                          uint32_t n, int32_t mode, rw_tree_im_storage* fallback_im,
                          rw_stream_t stream, rw_tree_learned_stats* stats);
-/* The MLP inputs of the 4,095 boundaries for d_keys (training data), the
- * window bases and spans, and the plain sample-quantile boundaries (host
- * arrays, any may be NULL: [4095*16], [4095], [4095], [4095]). */
+/* Training data: the MLP inputs of the 4,095 boundaries for d_keys under the
+ * current group size ([4095][16]; rows whose context does not fit inside the
+ * sample are zero and such boundaries stay sample quantiles) and the sorted
+ * sample ([65536]).  Host arrays, either may be NULL. */
 int rw_tree_learned_features(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
-                             float* features, uint32_t* window_lo, uint32_t* window_span,
-                             uint32_t* sample_quantiles, rw_stream_t stream);
+                             float* features, uint32_t* sorted_sample, rw_stream_t stream);
 /* Keys per bucket (host [4096]) under `mode`'s boundaries. */
 int rw_tree_learned_bucket_counts(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
                                   int32_t mode, uint32_t* counts, rw_stream_t stream);

@@ -26,7 +26,9 @@ __all__ = [
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "librw_tree.so")
+_BUILT_LIB = os.path.join(HERE, "librw_tree.so")
+# RW_TREE_LIBRARY names another build of the same C ABI (a debug build, say)
+LIB_PATH = os.environ.get("RW_TREE_LIBRARY", _BUILT_LIB)
 
 RW_OK, RW_ERR_ARG, RW_ERR_DEGENERATE, RW_ERR_CAPACITY = 0, 1, 2, 3
 RW_ERR_CUDA, RW_ERR_TIMEOUT, RW_ERR_NOT_READY, RW_ERR_NO_DEVICE = 4, 5, 6, 7
@@ -100,7 +102,9 @@ EXPORTS = (
     "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
     "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
+    "rw_tree_sort_profile",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
+    "rw_tree_learned_set_group",
     "rw_tree_learned_sort", "rw_tree_learned_features", "rw_tree_learned_bucket_counts",
     "rw_tree_mlp_param_count", "rw_tree_mlp_grad", "rw_tree_mlp_adam", "rw_tree_mlp_forward",
 )
@@ -330,6 +334,32 @@ run_stage1, run_stage2, run_stage3, run_stage4, run_stage5, run_stage6, run_stag
     _stage(k) for k in range(1, 8))
 
 
+def sort_keys(keys, out, im: ImStorage, stream=None) -> None:
+    """Onesweep sort of a device key tensor (int32 for 32-bit keys, int64 for
+    64-bit) into `out`, asynchronous on `stream` (rw_tree_sort_enqueue)."""
+    c = _AppDataC()
+    bits = 32 if keys.element_size() == 4 else 64
+    lib().rw_tree_app_data_init(ctypes.byref(c), ctypes.c_uint32(keys.numel()), ctypes.c_int32(bits))
+    c.u_morton_keys, c.u_morton_keys_alt = keys.data_ptr(), out.data_ptr()
+    _check(lib().rw_tree_sort_enqueue(ctypes.byref(c), im.handle, _stream_handle(stream)),
+           "sort_enqueue")
+
+
+def profile_sort(keys, out, im: ImStorage, reps: int = 5, stream=None) -> dict:
+    """Mean device milliseconds of the sort's kernels: histogram, sort_init,
+    sort_pass0 .. (rw_tree_sort_profile)."""
+    c = _AppDataC()
+    bits = 32 if keys.element_size() == 4 else 64
+    lib().rw_tree_app_data_init(ctypes.byref(c), ctypes.c_uint32(keys.numel()), ctypes.c_int32(bits))
+    c.u_morton_keys, c.u_morton_keys_alt = keys.data_ptr(), out.data_ptr()
+    ms = (ctypes.c_float * 64)()
+    nk = ctypes.c_int32()
+    _check(lib().rw_tree_sort_profile(ctypes.byref(c), im.handle, _stream_handle(stream), reps,
+                                      ms, 64, ctypes.byref(nk)), "sort_profile")
+    names = ["histogram", "sort_init"] + [f"sort_pass{p}" for p in range(nk.value - 2)]
+    return {names[i]: float(ms[i]) for i in range(nk.value)}
+
+
 def pipeline_enqueue(app: AppData, im: ImStorage, stream=None) -> None:
     _check(lib().rw_tree_pipeline_enqueue(ctypes.byref(app.c), im.handle,
                                           _stream_handle(stream)), "pipeline_enqueue")
@@ -435,8 +465,10 @@ class Batch:
         self.tuning = None
         if table and int(table["radix_bits"]) == (radix_bits or 8) and \
                 int(table["key_bits"]) == key_bits:
-            self.set_classes(autotune.class_list(table))
-            self.tuning = table
+            classes = autotune.class_list(table, sort_variants())
+            if classes is not None:
+                self.set_classes(classes)
+                self.tuning = table
 
     def capacity(self, c: int) -> int:
         return int(self.octree_offsets[c + 1] - self.octree_offsets[c])
@@ -535,23 +567,33 @@ class Learned:
     present, None leaves the network unset (sample quantiles only), or a
     float32 array of MLP_PARAMS values."""
 
-    def __init__(self, n_max: int, params="auto"):
+    def __init__(self, n_max: int, params="auto", group: int = 4):
         self._h = _vp()
         _check(lib().rw_tree_learned_create(ctypes.c_uint32(n_max), ctypes.byref(self._h)),
                "Learned")
         self.n_max = n_max
         self.params = None
+        self.group = group
         if isinstance(params, str) and params == "auto":
             from . import learned as _learned
-            params = _learned.load_params()
+            params, group = _learned.load_params(with_group=True)
         if params is not None:
-            self.set_params(params)
+            self.set_params(params, group)
+        else:
+            self.set_group(group)
 
-    def set_params(self, params) -> None:
+    def set_params(self, params, group: int | None = None) -> None:
         p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        g = self.group if group is None else int(group)
         _check(lib().rw_tree_learned_set_params(self._h, p.ctypes.data_as(_vp),
-                                                ctypes.c_int32(p.size)), "learned_set_params")
-        self.params = p
+                                                ctypes.c_int32(p.size), ctypes.c_int32(g)),
+               "learned_set_params")
+        self.params, self.group = p, g
+
+    def set_group(self, group: int) -> None:
+        _check(lib().rw_tree_learned_set_group(self._h, ctypes.c_int32(int(group))),
+               "learned_set_group")
+        self.group = int(group)
 
     def sort(self, keys, out=None, mode: int = LEARNED_MLP, fallback_im=None, stream=None):
         """Sorts a device int32 tensor of 32-bit keys; returns (sorted, stats)."""
@@ -567,17 +609,15 @@ class Learned:
                      "fell_back": st.fell_back}
 
     def features(self, keys, stream=None):
-        """MLP inputs [4095,16], window bases and spans, sample quantiles."""
+        """(MLP inputs [4095, 16] under the current group size, sorted sample
+        [65536] as uint32); rows whose context does not fit are zero."""
         n = keys.numel()
         f = np.zeros((4095, 16), np.float32)
-        lo = np.zeros(4095, np.uint32)
-        span = np.zeros(4095, np.uint32)
-        sq = np.zeros(4095, np.uint32)
+        srt = np.zeros(65536, np.uint32)
         _check(lib().rw_tree_learned_features(self._h, _dptr(keys), ctypes.c_uint32(n),
-                                              f.ctypes.data_as(_vp), lo.ctypes.data_as(_vp),
-                                              span.ctypes.data_as(_vp), sq.ctypes.data_as(_vp),
+                                              f.ctypes.data_as(_vp), srt.ctypes.data_as(_vp),
                                               _stream_handle(stream)), "learned_features")
-        return f, lo, span, sq
+        return f, srt
 
     def bucket_counts(self, keys, mode: int = LEARNED_MLP, stream=None) -> np.ndarray:
         c = np.zeros(4096, np.uint32)

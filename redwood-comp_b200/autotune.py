@@ -118,9 +118,29 @@ def load_table(key_bits: int) -> dict | None:
         return None
 
 
-def class_list(table: dict) -> list:
-    """[(max_points, variant)] for Batch.set_classes."""
-    return [(int(c["max_points"]), int(c["variant"])) for c in table["classes"]]
+def resolve_variant(entry: dict, key_bits: int, radix_bits: int, menu: list) -> int | None:
+    """Index in the current menu of the variant a table entry describes
+    (threads, keys per thread, ranking), or None when the menu lacks it.
+    Tables name variants by shape, so that adding menu entries does not
+    invalidate them."""
+    for v in menu:
+        if (v["key_bits"], v["radix_bits"], v["threads"], v["keys_per_thread"], v["rank"]) == \
+                (key_bits, radix_bits, int(entry["threads"]), int(entry["keys_per_thread"]),
+                 int(entry["rank"])):
+            return v["index"]
+    return None
+
+
+def class_list(table: dict, menu: list) -> list | None:
+    """[(max_points, variant index)] for Batch.set_classes, or None when a
+    class's variant is no longer in the menu."""
+    out = []
+    for c in table["classes"]:
+        idx = resolve_variant(c, int(table["key_bits"]), int(table["radix_bits"]), menu)
+        if idx is None:
+            return None
+        out.append((int(c["max_points"]), idx))
+    return out
 
 
 def main(argv=None) -> int:

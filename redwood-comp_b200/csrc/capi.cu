@@ -311,6 +311,44 @@ int rw_tree_sort_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im, rw_strea
   return RW_OK;
 }
 
+int rw_tree_sort_profile(rw_tree_app_data* app, rw_tree_im_storage* im, rw_stream_t stream,
+                         int32_t reps, float* kernel_ms, int32_t max_kernels,
+                         int32_t* n_kernels) {
+  if (int rc = check(app, im, kKeys | kAlt)) return rc;
+  if (!kernel_ms || reps < 1) return RW_ERR_ARG;
+  const int n_k = 2 + im->passes;  // histogram, sort_init, one per pass
+  if (max_kernels < n_k || n_k + 1 > 64) return RW_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const auto b = bufs_of(*app, im);
+  const auto sc = scratch_of(im);
+  const auto pl = plan_of(*app, im);
+  cudaEvent_t ev[64];
+  for (int i = 0; i <= n_k; ++i) RW_CUDA(cudaEventCreate(&ev[i]));
+  for (int i = 0; i < n_k; ++i) kernel_ms[i] = 0.0f;
+  int rc = RW_OK;
+  for (int r = 0; r < reps && rc == RW_OK; ++r) {
+    rc = clear_all(im, s);
+    if (rc != RW_OK) break;
+    cudaEventRecord(ev[0], s);
+    cudaError_t e = rwt::launch_keys(b, sc, pl, false, true, s);
+    cudaEventRecord(ev[1], s);
+    if (e == cudaSuccess) e = rwt::launch_sort_passes(b, sc, pl, s, ev + 2);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(e, "rw_tree_sort_profile");
+      break;
+    }
+    rc = sync_status(im, s);
+    for (int i = 0; rc == RW_OK && i < n_k; ++i) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      kernel_ms[i] += ms / float(reps);
+    }
+  }
+  for (int i = 0; i <= n_k; ++i) cudaEventDestroy(ev[i]);
+  if (n_kernels) *n_kernels = n_k;
+  return rc;
+}
+
 // ---- stage 3: unique (cu_dispatcher.cu:597-627) -------------------------------
 int rw_tree_run_stage3(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {

@@ -141,6 +141,9 @@ __device__ __forceinline__ void digit_exclusive_scan(const uint32_t* s_cnt,
   }
 }
 
+// Descriptors a look-back reads per round trip.
+constexpr int kLookback = 8;
+
 // Warp ranking schemes: all return, for each lane, the mask of valid lanes in
 // its warp holding the same digit (the lane's stable rank is the popcount of
 // the mask below it).
@@ -161,6 +164,7 @@ __device__ __forceinline__ uint32_t match_ballot(uint32_t digit, uint32_t valid_
 
 template <typename K, int D, int THREADS, int KPT, int RANK>
 struct BinCfg {
+  static_assert(32 * KPT < 65536, "warp ranks are packed in 16 bits");
   static constexpr int RADIX = 1 << D;
   static constexpr int NW = THREADS / 32;
   static constexpr int TILE = THREADS * KPT;
@@ -171,6 +175,63 @@ struct BinCfg {
       kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
   static_assert(kSmem <= 227 * 1024, "onesweep variant exceeds shared memory per CTA");
 };
+
+// Stable ranks of one warp's 32*KPT keys among the warp's keys of the same
+// digit (order: step, then lane); the warp's digit counters `wh` advance.
+// FULL: every key is in range, so no per-key checks are made.
+template <int D, int KPT, int RANK, bool FULL, typename K>
+__device__ __forceinline__ void warp_rank(const K (&keys)[KPT], uint32_t (&rank2)[(KPT + 1) / 2],
+                                          int shift, uint32_t wbase, uint32_t n, uint32_t* wh,
+                                          uint32_t* wm) {
+  constexpr uint32_t RADIX = 1u << D;
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const bool valid = FULL || wbase + 32u * i < n;
+    const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
+    uint32_t peers;
+    if (RANK == kRankBallot) {
+      peers = match_ballot<D>(dig, FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid));
+    } else if (RANK == kRankMatchAny) {
+      peers = __match_any_sync(0xffffffffu, valid ? dig : 0xffffffffu);
+      if (!valid) peers = 0;
+    } else {
+      if (valid) atomicOr(&wm[dig], 1u << lane);
+      __syncwarp();
+      peers = valid ? wm[dig] : 0u;
+      __syncwarp();
+    }
+    const uint32_t below = __popc(peers & lanemask_lt());
+    uint32_t prev = 0;
+    if (valid && below == 0) {
+      // one shared-memory access for the read-modify-write of the counter
+      prev = atomicAdd(&wh[dig], uint32_t(__popc(peers)));
+      if (RANK == kRankAtomicOr) wm[dig] = 0;
+    }
+    const int leader = valid ? __ffs(peers) - 1 : int(lane);
+    prev = __shfl_sync(0xffffffffu, prev, leader);
+    const uint32_t r = prev + below;
+    if (i & 1) rank2[i >> 1] |= r << 16;
+    else rank2[i >> 1] = r;
+    __syncwarp();
+  }
+}
+
+// Places the warp's keys at their tile positions (wh: the warp's offsets).
+template <int D, int KPT, bool FULL, typename K>
+__device__ __forceinline__ void warp_place(const K (&keys)[KPT],
+                                           const uint32_t (&rank2)[(KPT + 1) / 2], int shift,
+                                           uint32_t wbase, uint32_t n, const uint32_t* wh,
+                                           K* s_keys) {
+  constexpr uint32_t RADIX = 1u << D;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    if (FULL || wbase + 32u * i < n) {
+      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
+      s_keys[wh[dig] + ((rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu)] = keys[i];
+    }
+  }
+}
 
 // One onesweep pass over `n` keys: digit `shift`..`shift+D-1`, stable.
 // desc: [(tiles + 1) x RADIX] descriptors, row 0 prefilled with the global
@@ -194,9 +255,11 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   if (tid == 0) s_misc[0] = atomicAdd(tile_ctr, 1u);
-  for (int i = tid; i < NW * RADIX; i += THREADS) {
-    s_hist[i] = 0;
-    if (RANK == kRankAtomicOr) s_match[i] = 0;
+  {
+    static_assert((NW * RADIX) % 4 == 0 && C::kKeysBytes % 16 == 0, "16-byte zeroing");
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    constexpr int kWords = (RANK == kRankAtomicOr ? 2 : 1) * NW * RADIX;  // s_hist, s_match
+    for (int i = tid; i < kWords / 4; i += THREADS) reinterpret_cast<uint4*>(s_hist)[i] = z;
   }
   __syncthreads();
   const uint32_t tile = s_misc[0];
@@ -204,55 +267,31 @@ __global__ void __launch_bounds__(THREADS, MINB)
   const uint32_t segc = tile_segment(seg, map, tile, &first_tile);
   const uint32_t base = seg_begin(seg, segc) + (tile - first_tile) * TILE;
   const uint32_t n = seg_begin(seg, segc) + seg_size(seg, segc);  // end of the segment
-  const uint32_t row = tile + segc + 1;       // this tile's descriptor row
-  const uint32_t init_row = first_tile + segc;  // the segment's inclusive row
+  const int row = int(tile + segc + 1);       // this tile's descriptor row
+  const int init_row = int(first_tile + segc);  // the segment's inclusive row
+  const bool full = base + TILE <= n;
 
   // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
   K keys[KPT];
-  uint32_t rank[KPT];
+  uint32_t rank2[(KPT + 1) / 2];  // warp ranks (< 32 * KPT), two per register
   const uint32_t wbase = base + warp * 32u * KPT + lane;
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    const uint32_t idx = wbase + 32u * i;
-    keys[i] = idx < n ? in[idx] : K(0);
-  }
-
-  // per-warp stable ranks (key order inside the warp = step, then lane)
   uint32_t* wh = s_hist + warp * RADIX;
   uint32_t* wm = s_match + warp * RADIX;
+  if (full) {
 #pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    const uint32_t idx = wbase + 32u * i;
-    const bool valid = idx < n;
-    const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-    uint32_t peers;
-    if (RANK == kRankBallot) {
-      peers = match_ballot<D>(dig, __ballot_sync(0xffffffffu, valid));
-    } else if (RANK == kRankMatchAny) {
-      peers = __match_any_sync(0xffffffffu, valid ? dig : 0xffffffffu);
-      if (!valid) peers = 0;
-    } else {
-      if (valid) atomicOr(&wm[dig], 1u << lane);
-      __syncwarp();
-      peers = valid ? wm[dig] : 0u;
+    for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
+    warp_rank<D, KPT, RANK, true>(keys, rank2, shift, wbase, n, wh, wm);
+  } else {
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      const uint32_t idx = wbase + 32u * i;
+      keys[i] = idx < n ? in[idx] : K(0);
     }
-    const uint32_t below = __popc(peers & lanemask_lt());
-    uint32_t prev = 0;
-    if (RANK == kRankAtomicOr) __syncwarp();
-    if (valid && below == 0) {
-      prev = wh[dig];
-      wh[dig] = prev + __popc(peers);
-      if (RANK == kRankAtomicOr) wm[dig] = 0;
-    }
-    const int leader = valid ? __ffs(peers) - 1 : int(lane);
-    prev = __shfl_sync(0xffffffffu, prev, leader);
-    rank[i] = prev + below;
-    __syncwarp();
+    warp_rank<D, KPT, RANK, false>(keys, rank2, shift, wbase, n, wh, wm);
   }
   __syncthreads();
 
-  // per digit: exclusive scan over warps, publish the tile aggregate, then
-  // look back at once so the inclusive prefix is out as early as possible
+  // per digit: exclusive scan over warps and publish the tile aggregate
   uint32_t* drow = desc + size_t(row) * RADIX;
   for (int d = tid; d < RADIX; d += THREADS) {
     uint32_t run = 0;
@@ -265,34 +304,45 @@ __global__ void __launch_bounds__(THREADS, MINB)
     s_cnt[d] = run;
     st_relaxed(drow + d, kFlagAgg | (run << 2));
   }
+  __syncthreads();
+  digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
+  __syncthreads();
+  // fold the digit starts into the per-warp offsets once per tile, so that
+  // placing a key below reads one shared-memory word instead of two
+  for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] += s_start[i & (RADIX - 1)];
+  __syncthreads();
+
+  // reorder the tile by digit in shared memory first: it needs only the
+  // tile's own counts, and gives the predecessors time to publish their
+  // inclusive prefixes before the look-back below reads them
+  if (full) warp_place<D, KPT, true>(keys, rank2, shift, wbase, n, wh, s_keys);
+  else warp_place<D, KPT, false>(keys, rank2, shift, wbase, n, wh, s_keys);
+
+  // decoupled look-back, kLookback descriptors per round trip.  The segment's
+  // first row is always inclusive, so rows are read clamped to it and the
+  // walk stops there at the latest.
   for (int d = tid; d < RADIX; d += THREADS) {
-    // walk back 4 descriptors per round trip; row 0 is always inclusive
     uint32_t excl = 0;
-    int64_t k = row - 1;  // the predecessor's row; the init row is inclusive
+    int k = row - 1;
     uint32_t spin = 0;
     while (true) {
-      uint32_t v[4];
+      uint32_t v[kLookback];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        v[q] = k - q >= int64_t(init_row) ? ld_relaxed(desc + size_t(k - q) * RADIX + d)
-                                          : kFlagInc;
-      bool done = false;
+      for (int q = 0; q < kLookback; ++q)
+        v[q] = ld_relaxed(desc + size_t(max(k - q, init_row)) * RADIX + d);
       int used = 0;
+      bool done = false;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (done || used != q) break;
+      for (int q = 0; q < kLookback; ++q) {
         const uint32_t f = v[q] & kFlagMask;
-        if (f == kFlagInc) {
-          excl += v[q] >> 2;
-          done = true;
-        } else if (f == kFlagAgg) {
-          excl += v[q] >> 2;
-          ++used;
-        }
+        if (done || f == 0 || used != q) break;
+        excl += v[q] >> 2;
+        ++used;
+        done = f == kFlagInc;
       }
       if (done) break;
-      k -= used;
       if (used) {
+        k -= used;
         spin = 0;
         continue;
       }
@@ -303,31 +353,28 @@ __global__ void __launch_bounds__(THREADS, MINB)
       backoff(spin);
     }
     st_relaxed(drow + d, kFlagInc | ((excl + s_cnt[d]) << 2));
-    s_gofs[d] = excl;
+    s_gofs[d] = excl - s_start[d];
   }
   __syncthreads();
-  digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
-  __syncthreads();
 
-  // reorder the tile by digit in shared memory
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    const uint32_t idx = wbase + 32u * i;
-    if (idx < n) {
-      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-      s_keys[s_start[dig] + wh[dig] + rank[i]] = keys[i];
+  // write runs of equal digits to their global positions (a destination is
+  // out of range only if a look-back gave up)
+  const uint32_t total = seg.total;
+  if (full) {
+#pragma unroll 4
+    for (int i = 0; i < KPT; ++i) {
+      const uint32_t p = tid + uint32_t(i) * THREADS;
+      const K k = s_keys[p];
+      const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
+      if (dst < total) out[dst] = k;
     }
-  }
-  for (int d = tid; d < RADIX; d += THREADS) s_gofs[d] -= s_start[d];
-  __syncthreads();
-
-  // write runs of equal digits to their global positions
-  const uint32_t tile_n = min(uint32_t(TILE), n - base);
-  for (uint32_t p = tid; p < tile_n; p += THREADS) {
-    const K k = s_keys[p];
-    const uint32_t dig = uint32_t(k >> shift) & (RADIX - 1);
-    const uint32_t dst = s_gofs[dig] + p;
-    if (dst < seg.total) out[dst] = k;  // always true unless a look-back gave up
+  } else {
+    const uint32_t tile_n = n - base;
+    for (uint32_t p = tid; p < tile_n; p += THREADS) {
+      const K k = s_keys[p];
+      const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
+      if (dst < total) out[dst] = k;
+    }
   }
 }
 
@@ -406,19 +453,27 @@ struct SortVariant {
 // The menu the autotuner chooses from (entry 0 of each key/digit width is
 // the default).
 const SortVariant kVariants[] = {
+    {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 2>},
     {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 2>},
     {32, 8, 384, 16, kRankAtomicOr, passes_t<uint32_t, 8, 384, 16, kRankAtomicOr, 2>},
     {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 3>},
     {32, 8, 256, 24, kRankAtomicOr, passes_t<uint32_t, 8, 256, 24, kRankAtomicOr, 2>},
-    {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 2>},
     {32, 8, 512, 24, kRankAtomicOr, passes_t<uint32_t, 8, 512, 24, kRankAtomicOr, 1>},
     {32, 8, 256, 16, kRankBallot, passes_t<uint32_t, 8, 256, 16, kRankBallot, 3>},
     {32, 8, 512, 16, kRankBallot, passes_t<uint32_t, 8, 512, 16, kRankBallot, 1>},
     {32, 8, 384, 16, kRankMatchAny, passes_t<uint32_t, 8, 384, 16, kRankMatchAny, 2>},
+    {32, 8, 512, 16, kRankBallot, passes_t<uint32_t, 8, 512, 16, kRankBallot, 2>},
+    {32, 8, 384, 16, kRankBallot, passes_t<uint32_t, 8, 384, 16, kRankBallot, 2>},
+    {32, 8, 256, 32, kRankBallot, passes_t<uint32_t, 8, 256, 32, kRankBallot, 2>},
+    {32, 8, 512, 16, kRankMatchAny, passes_t<uint32_t, 8, 512, 16, kRankMatchAny, 2>},
+    {32, 8, 1024, 16, kRankAtomicOr, passes_t<uint32_t, 8, 1024, 16, kRankAtomicOr, 1>},
+    {32, 8, 1024, 8, kRankAtomicOr, passes_t<uint32_t, 8, 1024, 8, kRankAtomicOr, 1>},
     {32, 11, 512, 16, kRankBallot, passes_t<uint32_t, 11, 512, 16, kRankBallot, 1>},
     {32, 11, 256, 16, kRankAtomicOr, passes_t<uint32_t, 11, 256, 16, kRankAtomicOr, 1>},
     {32, 11, 256, 24, kRankAtomicOr, passes_t<uint32_t, 11, 256, 24, kRankAtomicOr, 1>},
     {32, 11, 256, 24, kRankBallot, passes_t<uint32_t, 11, 256, 24, kRankBallot, 1>},
+    {32, 11, 256, 16, kRankBallot, passes_t<uint32_t, 11, 256, 16, kRankBallot, 2>},
+    {32, 11, 384, 16, kRankBallot, passes_t<uint32_t, 11, 384, 16, kRankBallot, 1>},
     {64, 8, 384, 16, kRankAtomicOr, passes_t<uint64_t, 8, 384, 16, kRankAtomicOr, 2>},
     {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},
     {64, 8, 256, 12, kRankAtomicOr, passes_t<uint64_t, 8, 256, 12, kRankAtomicOr, 3>},

@@ -2,12 +2,17 @@
 // reference sorts with an LSD radix sort only).
 //
 //  1. a stratified 64K-key sample of the input, sorted with the onesweep sort;
-//  2. 4,095 bucket boundaries: boundary j looks at the 16 sorted sample keys
-//     around sample rank 16(j+1) and places itself inside that window, either
-//     by the MLP (mlp.cuh) or, without the network, at the window's middle key
-//     (the plain sample quantile).  Windows are disjoint and ordered and the
-//     boundary is clamped into its window, so boundaries never decrease;
-//  3. bucket(k) = number of boundaries <= k, a non-decreasing function, so
+//  2. 4,095 bucket boundaries.  Without the network boundary j is the sample
+//     key of rank c = 16(j+1) (the plain sample quantile).  With it, the MLP
+//     (mlp.cuh) reads a context of 16g sorted sample keys centred on c (eight
+//     inputs: mean positions of eight groups of 2g keys; eight more: the exact
+//     positions of the keys of ranks c-4 .. c+3; all normalised to the
+//     context's key range) and returns the boundary's offset from c in sample
+//     ranks; the key is interpolated between the two sample keys around that
+//     fractional rank.  This is a smoothed inversion of the sample's CDF that
+//     averages the sampling noise of the whole context instead of taking one
+//     order statistic.  A prefix maximum then makes the boundaries
+//     non-decreasing;//  3. bucket(k) = number of boundaries <= k, a non-decreasing function, so
 //     sorting every bucket and concatenating them sorts the input;
 //  4. one histogram pass, a plan (offsets, overflow), one scatter pass;
 //  5. one CTA per bucket sorts it in shared memory (stable LSD over only the
@@ -63,12 +68,36 @@ __global__ void k_sample(const uint32_t* __restrict__ keys, uint32_t n,
   sample[i] = keys[pos];
 }
 
-// 2. boundaries (and, for training, the MLP inputs of every boundary)
+// Context group sizes the boundary MLP accepts (context = 16 * group keys).
+constexpr uint32_t kMaxGroup = 16;
+
+// MLP inputs of boundary j (sample rank c, context [c - half, c + half)).
+__device__ __forceinline__ void boundary_features(const uint32_t* __restrict__ s, uint32_t c,
+                                                  uint32_t half, uint32_t group,
+                                                  float (&x)[kMlpIn]) {
+  const uint32_t* ctx = s + (c - half);
+  const uint32_t lo = ctx[0], span = max(ctx[2 * half - 1] - lo, 1u);
+  const uint32_t g2 = 2 * group;  // keys per coarse group
+  const float fspan = float(span);
+  const float denom = __fmul_rn(float(g2), fspan);
+#pragma unroll
+  for (int i = 0; i < kMlpIn / 2; ++i) {
+    uint64_t sum = 0;
+    for (uint32_t q = 0; q < g2; ++q) sum += ctx[i * g2 + q] - lo;
+    x[i] = __fdiv_rn(__ull2float_rn(sum), denom);
+  }
+#pragma unroll
+  for (int i = 0; i < kMlpIn / 2; ++i)
+    x[kMlpIn / 2 + i] = __fdiv_rn(float(s[c - kMlpIn / 4 + i] - lo), fspan);
+}
+
+// 2. boundaries (and, for training, the MLP inputs of every boundary; rows
+// whose context does not fit inside the sample are written as zeros and keep
+// the sample quantile).  MLP boundaries still need k_bounds_monotone.
 template <bool USE_MLP>
 __global__ void __launch_bounds__(256)
     k_boundaries(const uint32_t* __restrict__ sorted_sample, const float* __restrict__ params,
-                 uint32_t* __restrict__ bounds, float* __restrict__ features,
-                 uint32_t* __restrict__ win_lo, uint32_t* __restrict__ win_span) {
+                 uint32_t group, uint32_t* __restrict__ bounds, float* __restrict__ features) {
   __shared__ float s_w1[kMlpHidden * kMlpIn], s_w2[kMlpHidden * kMlpHidden], s_w3[kMlpHidden],
       s_b1[kMlpHidden], s_b2[kMlpHidden];
   if (USE_MLP) {
@@ -88,50 +117,106 @@ __global__ void __launch_bounds__(256)
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= kBounds) return;
   const uint32_t c = (j + 1) * kSpacing;  // sample rank of the ideal boundary
-  const uint32_t* w = sorted_sample + (c - kSpacing / 2);
-  const uint32_t lo = w[0], hi = w[kSpacing - 1];
-  const uint32_t span = max(hi - lo, 1u);
-  float x[kMlpIn];
+  const uint32_t half = (kMlpIn / 2) * group;
+  const bool fits = c >= half && c + half <= kSample;
+  uint32_t b = sorted_sample[c];
+  if ((USE_MLP || features) && fits) {
+    float x[kMlpIn];
+    boundary_features(sorted_sample, c, half, group, x);
+    if (features) {
 #pragma unroll
-  for (int i = 0; i < kMlpIn; ++i) x[i] = __fdiv_rn(float(w[i] - lo), float(span));
-  if (features) {
+      for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = x[i];
+    }
+    if (USE_MLP) {
+      // offset in sample ranks, d in [-half, half - 1]
+      const float y = mlp_eval(x, s_w1, s_b1, s_w2, s_b2, s_w3, params[kMlpParams - 1]);
+      const float fh = float(half);
+      const float d = fminf(fmaxf(__fmul_rn(y, fh), -fh), fh - 1.0f);
+      const float fl = floorf(d);
+      const uint32_t i0 = uint32_t(int(c) + int(fl));
+      const uint32_t i1 = min(i0 + 1, kSample - 1);
+      const uint32_t a0 = sorted_sample[i0], gap = sorted_sample[i1] - a0;
+      b = a0 + min(uint32_t(__fmul_rn(d - fl, float(gap)) + 0.5f), gap);
+    }
+  } else if (features) {
 #pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = x[i];
-    win_lo[j] = lo;
-    win_span[j] = span;
-  }
-  uint32_t b;
-  if (USE_MLP) {
-    const float y = mlp_eval(x, s_w1, s_b1, s_w2, s_b2, s_w3, params[kMlpParams - 1]);
-    const float yc = fminf(fmaxf(y, 0.0f), 1.0f);
-    const uint32_t off = uint32_t(__fmul_rn(yc, float(hi - lo)) + 0.5f);
-    b = lo + min(off, hi - lo);
-  } else {
-    b = w[kSpacing / 2];
+    for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = 0.0f;
   }
   bounds[j] = b;
 }
 
-// bucket of key k: number of boundaries <= k (boundaries in shared memory)
-__device__ __forceinline__ uint32_t bucket_of(const uint32_t* s_b, uint32_t k) {
-  uint32_t lo = 0, hi = kBounds;
+// prefix maximum over the boundaries (one block): non-decreasing boundaries
+// are what makes "bucket = number of boundaries <= key" order-preserving
+__global__ void __launch_bounds__(1024) k_bounds_monotone(uint32_t* __restrict__ bounds) {
+  __shared__ uint32_t s_warp[32];
+  constexpr int R = kBuckets / 1024;
+  const int first = threadIdx.x * R;
+  uint32_t v[R], mx = 0;
 #pragma unroll
-  for (int it = 0; it < 12; ++it) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (lo < hi) {
-      if (s_b[mid] <= k) lo = mid + 1;
-      else hi = mid;
-    }
+  for (int r = 0; r < R; ++r) {
+    v[r] = first + r < int(kBounds) ? bounds[first + r] : 0u;
+    mx = max(mx, v[r]);
   }
-  return lo;
+  // inclusive max-scan of the per-thread maxima
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t inc = mx;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (int(lane) >= d) inc = max(inc, o);
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = s_warp[lane];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, w, d);
+      if (int(lane) >= d) w = max(w, o);
+    }
+    s_warp[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) run = 0;
+  if (warp > 0) run = max(run, s_warp[warp - 1]);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    run = max(run, v[r]);
+    if (first + r < int(kBounds)) bounds[first + r] = run;
+  }
+}
+
+// Splitter tree (Sanders & Winkel, "Super Scalar Sample Sort", ESA 2004): the
+// 4,095 sorted boundaries in breadth-first order, t[1] the median, children of
+// node i at 2i and 2i+1.  A descent reads one node per level; the five top
+// levels are 31 consecutive words (no bank conflicts between lanes), where a
+// binary search over the sorted array would put its top levels in one bank.
+// t[0] is unused.
+__device__ __forceinline__ void load_tree(const uint32_t* __restrict__ bounds, uint32_t* s_t) {
+  constexpr int kLevels = 12;
+  static_assert((1u << kLevels) == kBuckets, "complete tree");
+  for (int i = threadIdx.x + 1; i < int(kBuckets); i += blockDim.x) {
+    const int d = 31 - __clz(i);   // depth of node i
+    const int p = i - (1 << d);    // position in its level
+    s_t[i] = bounds[((2 * p + 1) << (kLevels - 1 - d)) - 1];
+  }
+}
+
+// bucket of key k: number of boundaries <= k
+__device__ __forceinline__ uint32_t bucket_of(const uint32_t* s_t, uint32_t k) {
+  uint32_t i = 1;
+#pragma unroll
+  for (int it = 0; it < 12; ++it) i = 2 * i + (k >= s_t[i] ? 1u : 0u);
+  return i - kBuckets;
 }
 
 // 4a. histogram of the buckets
 __global__ void __launch_bounds__(512)
     k_bucket_hist(const uint32_t* __restrict__ keys, uint32_t n,
                   const uint32_t* __restrict__ bounds, uint32_t* __restrict__ counts) {
-  __shared__ uint32_t s_b[kBounds], s_cnt[kBuckets];
-  for (int i = threadIdx.x; i < int(kBounds); i += blockDim.x) s_b[i] = bounds[i];
+  __shared__ uint32_t s_b[kBuckets], s_cnt[kBuckets];
+  load_tree(bounds, s_b);
   for (int i = threadIdx.x; i < int(kBuckets); i += blockDim.x) s_cnt[i] = 0;
   __syncthreads();
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -182,13 +267,13 @@ __global__ void __launch_bounds__(kScThreads)
                      uint32_t* __restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
   uint32_t* s_keys = sm;                  // [kScTile]
-  uint32_t* s_b = s_keys + kScTile;       // [kBounds] (+1 pad)
+  uint32_t* s_b = s_keys + kScTile;       // [kBuckets] splitter tree
   uint32_t* s_cnt = s_b + kBuckets;       // [kBuckets] counts, then global bases
   uint32_t* s_pos = s_cnt + kBuckets;     // [kBuckets] starts, then fill cursors
   uint32_t* s_start = s_pos + kBuckets;   // [kBuckets]
   uint16_t* s_bid = reinterpret_cast<uint16_t*>(s_start + kBuckets);  // [kScTile]
   uint32_t* s_warp = reinterpret_cast<uint32_t*>(s_bid + kScTile);    // [kScThreads/32+1]
-  for (int i = threadIdx.x; i < int(kBounds); i += kScThreads) s_b[i] = bounds[i];
+  load_tree(bounds, s_b);
   for (int i = threadIdx.x; i < int(kBuckets); i += kScThreads) s_cnt[i] = 0;
   __syncthreads();
   const uint32_t base = blockIdx.x * kScTile;
@@ -533,11 +618,12 @@ struct rw_tree_learned {
   void* d_mem = nullptr;
   uint32_t *d_sample = nullptr, *d_sample_sorted = nullptr, *d_bounds = nullptr,
            *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr,
-           *d_tmp = nullptr, *d_win_lo = nullptr, *d_win_span = nullptr;
+           *d_tmp = nullptr;
   float* d_params = nullptr;
   float* d_features = nullptr;
   rwt::LearnedPlan* d_plan = nullptr;
   rwt::LearnedPlan* h_plan = nullptr;
+  uint32_t group = 4;  // sample keys per MLP input
   bool has_params = false;
 };
 
@@ -567,12 +653,14 @@ int boundaries(rw_tree_learned* L, bool mlp, bool features, cudaStream_t s) {
   if (mlp && !L->has_params) return RW_ERR_NOT_READY;
   float* f = features ? L->d_features : nullptr;
   const uint32_t blocks = (rwt::kBounds + 255) / 256;
-  if (mlp)
-    rwt::k_boundaries<true><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params, L->d_bounds,
-                                                   f, L->d_win_lo, L->d_win_span);
-  else
-    rwt::k_boundaries<false><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params,
-                                                    L->d_bounds, f, L->d_win_lo, L->d_win_span);
+  if (mlp) {
+    rwt::k_boundaries<true><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params, L->group,
+                                                   L->d_bounds, f);
+    RWL_CUDA(cudaGetLastError());
+    rwt::k_bounds_monotone<<<1, 1024, 0, s>>>(L->d_bounds);
+  } else
+    rwt::k_boundaries<false><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params, L->group,
+                                                    L->d_bounds, f);
   RWL_CUDA(cudaGetLastError());
   return RW_OK;
 }
@@ -615,8 +703,9 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
     return rc;
   }
   const size_t words = 2 * size_t(rwt::kSample) + rwt::kBuckets + rwt::kBuckets +
-                       (rwt::kBuckets + 1) + rwt::kBuckets + size_t(n_max) + 2 * rwt::kBuckets +
-                       rwt::kMlpParams + size_t(rwt::kBounds) * rwt::kMlpIn + 64;
+                       (rwt::kBuckets + 1) + rwt::kBuckets + size_t(n_max) +
+                       rwt::kMlpParams + size_t(rwt::kBounds) * rwt::kMlpIn +
+                       64 /* alignment of the plan */ + 64 /* plan */;
   cudaError_t e = cudaMalloc(&L->d_mem, 4 * words);
   if (e == cudaSuccess) e = cudaMallocHost(&L->h_plan, sizeof(rwt::LearnedPlan));
   if (e != cudaSuccess) {
@@ -630,8 +719,6 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
   L->d_counts = p; p += rwt::kBuckets;
   L->d_offsets = p; p += rwt::kBuckets + 1;
   L->d_cursor = p; p += rwt::kBuckets;
-  L->d_win_lo = p; p += rwt::kBuckets;
-  L->d_win_span = p; p += rwt::kBuckets;
   L->d_params = reinterpret_cast<float*>(p); p += rwt::kMlpParams;
   L->d_features = reinterpret_cast<float*>(p); p += size_t(rwt::kBounds) * rwt::kMlpIn;
   p = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(p) + 255) & ~uintptr_t(255));
@@ -660,27 +747,31 @@ int rw_tree_learned_destroy(rw_tree_learned* L) {
   return RW_OK;
 }
 
-int rw_tree_learned_set_params(rw_tree_learned* L, const float* params, int32_t count) {
+int rw_tree_learned_set_params(rw_tree_learned* L, const float* params, int32_t count,
+                               int32_t group) {
   if (!L || !params || count != rwt::kMlpParams) return RW_ERR_ARG;
+  if (int rc = rw_tree_learned_set_group(L, group)) return rc;
   RWL_CUDA(cudaMemcpy(L->d_params, params, 4 * size_t(count), cudaMemcpyHostToDevice));
   L->has_params = true;
   return RW_OK;
 }
 
+int rw_tree_learned_set_group(rw_tree_learned* L, int32_t group) {
+  if (!L || group < 1 || uint32_t(group) > rwt::kMaxGroup || (group & (group - 1))) return RW_ERR_ARG;
+  L->group = uint32_t(group);
+  return RW_OK;
+}
+
 int rw_tree_learned_features(rw_tree_learned* L, const uint32_t* d_keys, uint32_t n,
-                             float* h_features, uint32_t* h_lo, uint32_t* h_span,
-                             uint32_t* h_sample_quantiles, rw_stream_t stream) {
+                             float* h_features, uint32_t* h_sorted_sample, rw_stream_t stream) {
   if (!L || !d_keys || n < rwt::kSample || n > L->n_max) return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = front_half(L, d_keys, n, false, true, s)) return rc;
   if (h_features)
     RWL_CUDA(cudaMemcpyAsync(h_features, L->d_features,
                              4 * size_t(rwt::kBounds) * rwt::kMlpIn, cudaMemcpyDeviceToHost, s));
-  if (h_lo) RWL_CUDA(cudaMemcpyAsync(h_lo, L->d_win_lo, 4 * rwt::kBounds, cudaMemcpyDeviceToHost, s));
-  if (h_span)
-    RWL_CUDA(cudaMemcpyAsync(h_span, L->d_win_span, 4 * rwt::kBounds, cudaMemcpyDeviceToHost, s));
-  if (h_sample_quantiles)
-    RWL_CUDA(cudaMemcpyAsync(h_sample_quantiles, L->d_bounds, 4 * rwt::kBounds,
+  if (h_sorted_sample)
+    RWL_CUDA(cudaMemcpyAsync(h_sorted_sample, L->d_sample_sorted, 4 * size_t(rwt::kSample),
                              cudaMemcpyDeviceToHost, s));
   RWL_CUDA(cudaStreamSynchronize(s));
   return RW_OK;

@@ -63,9 +63,9 @@ def _keys(rw, n, kind, seed):
 def test_learned_sort_equals_plain_sort(rw, n):
     torch = _torch()
     from redwood_comp_b200 import learned
-    L = rw.Learned(n, params=None)
-    L.set_params(learned.load_params() if learned.load_params() is not None
-                 else learned.init_params(1))
+    L = rw.Learned(n)  # the trained table and its group size, when present
+    if L.params is None:
+        L.set_params(learned.init_params(1))
     im = rw.ImStorage(n, 32)
     for kind in ("gauss", "uniform"):
         keys = _keys(rw, n, kind, 41 + n % 97)
@@ -95,3 +95,41 @@ def test_learned_sort_large_bucket_and_fallback(rw):
     out, st = L.sort(same, mode=rw.LEARNED_SAMPLE_QUANTILES, fallback_im=im)
     assert st["fell_back"] == 1
     assert bool((out == 77).all())
+
+
+@pytest.mark.parametrize("group", [1, 2, 16])
+def test_learned_sort_exact_for_every_group(rw, group):
+    """Untrained weights and every context width: boundaries stay monotone
+    (the clamp), so the output is still exactly sorted."""
+    from redwood_comp_b200 import learned
+    n = 1_000_003
+    L = rw.Learned(n, params=learned.init_params(5), group=group)
+    im = rw.ImStorage(n, 32)
+    keys = _keys(rw, n, "gauss", 77)
+    out, st = L.sort(keys, mode=rw.LEARNED_MLP, fallback_im=im)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32),
+                          np.sort(keys.cpu().numpy().view(np.uint32)))
+
+
+@pytest.mark.parametrize("group", [1, 4, 16])
+def test_features_match_numpy_restatement(rw, group):
+    """The kernel's MLP inputs equal a float64 restatement from the sorted
+    sample it returns: mean positions of eight groups of 2g context keys, then
+    the positions of the keys of ranks c-4 .. c+3, normalised to the context."""
+    from redwood_comp_b200 import learned
+    n = 1 << 20
+    L = rw.Learned(n, params=None, group=group)
+    keys = _keys(rw, n, "gauss", 13)
+    f, sample = L.features(keys)
+    assert np.all(np.diff(sample.astype(np.int64)) >= 0)
+    assert np.isin(sample, keys.cpu().numpy().view(np.uint32)).all()
+    rows, c, half = learned.context_rows(group)
+    s = sample.astype(np.float64)
+    lo = s[c - half]
+    span = np.maximum(s[c + half - 1] - lo, 1.0)
+    ctx = np.stack([s[c - half + i] for i in range(2 * half)], 1) - lo[:, None]
+    coarse = ctx.reshape(len(rows), 8, 2 * group).mean(2) / span[:, None]
+    fine = (np.stack([s[c - 4 + i] for i in range(8)], 1) - lo[:, None]) / span[:, None]
+    np.testing.assert_allclose(f[rows], np.concatenate([coarse, fine], 1), rtol=4e-7, atol=1e-7)
+    others = np.setdiff1d(np.arange(4095), rows)
+    assert np.all(f[others] == 0)
