@@ -293,13 +293,13 @@ int rw_tree_sort_profile(rw_tree_app_data* app, rw_tree_im_storage* im, rw_strea
  * bucket boundaries are placed, one per 16 sample ranks: at the sample key of
  * rank 16(j+1) (plain sample quantiles, the method without the network), or
  * by the boundary MLP (16 -> 64 -> 64 -> 1, BF16 weights, FP32 accumulate),
- * which reads a context of 16 groups of `group` sorted sample keys around that
- * rank (input i = mean position of group i inside the context's key range)
- * and returns the boundary's position in that range; it is clamped into the
- * boundary's own 16 sample ranks, so boundaries never decrease.  Keys are
- * scattered into the 4,096 buckets in one pass and each bucket is sorted
- * exactly.  A bucket larger than 2^21 keys sends the whole input to the
- * onesweep sort.  The output is the sorted input either way. */
+ * which reads a context of 16*group sorted sample keys around that rank and
+ * returns the boundary's offset from it in sample ranks; a prefix maximum
+ * keeps the boundaries non-decreasing.  Keys are scattered into the 4,096
+ * buckets in one pass, every bucket into a region of 4x the mean bucket size,
+ * and each bucket is sorted exactly.  A bucket that overflows its region
+ * sends the whole input to the onesweep sort.  The output is the sorted input
+ * either way. */
 typedef struct rw_tree_learned rw_tree_learned;
 #define RW_LEARNED_MLP 0
 #define RW_LEARNED_SAMPLE_QUANTILES 1
@@ -308,12 +308,13 @@ typedef struct rw_tree_learned rw_tree_learned;
 
 typedef struct rw_tree_learned_stats {
   uint32_t max_bucket;  /* keys in the fullest bucket */
-  uint32_t big_buckets; /* buckets sorted by the chunked single-CTA path */
-  uint32_t fell_back;   /* 1 when the onesweep sort ran instead */
+  uint32_t big_buckets; /* buckets above one CTA's 32,768 keys (chunked path) */
+  uint32_t fell_back;   /* 1 when a bucket overflowed and the onesweep sort ran */
   uint32_t reserved;
 } rw_tree_learned_stats;
 
-/* Scratch for inputs of up to n_max (>= 65536) keys on the current device. */
+/* Scratch for inputs of up to n_max (>= 65536) keys on the current device
+ * (about 16 bytes per key of n_max, for the bucket regions). */
 int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out);
 int rw_tree_learned_destroy(rw_tree_learned* learned);
 /* FP32 master parameters (RW_LEARNED_MLP_PARAMS floats, layout W1[64][16],
@@ -323,9 +324,9 @@ int rw_tree_learned_set_params(rw_tree_learned* learned, const float* params, in
                                int32_t group);
 /* Context group size alone (for rw_tree_learned_features); default 4. */
 int rw_tree_learned_set_group(rw_tree_learned* learned, int32_t group);
-/* Sorts d_keys[0, n) into d_sorted.  `fallback_im` (storage for n keys) runs
- * the onesweep sort when needed; stats may be NULL.  Synchronises once (the
- * bucket plan decides the path). */
+/* Sorts d_keys[0, n) (16-byte aligned) into d_sorted.  `fallback_im`
+ * (storage for n keys) runs the onesweep sort when needed; stats may be NULL.
+ * Synchronises once (the bucket plan decides the path). */
 int rw_tree_learned_sort(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t* d_sorted,
                          uint32_t n, int32_t mode, rw_tree_im_storage* fallback_im,
                          rw_stream_t stream, rw_tree_learned_stats* stats);
@@ -335,7 +336,8 @@ int rw_tree_learned_sort(rw_tree_learned* learned, const uint32_t* d_keys, uint3
  * sample ([65536]).  Host arrays, either may be NULL. */
 int rw_tree_learned_features(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
                              float* features, uint32_t* sorted_sample, rw_stream_t stream);
-/* Keys per bucket (host [4096]) under `mode`'s boundaries. */
+/* Keys per bucket (host [4096]) under `mode`'s boundaries (d_keys 16-byte
+ * aligned). */
 int rw_tree_learned_bucket_counts(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
                                   int32_t mode, uint32_t* counts, rw_stream_t stream);
 

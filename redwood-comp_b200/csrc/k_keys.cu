@@ -17,6 +17,7 @@
 
 #include "internal.hpp"
 #include "morton.cuh"
+#include "rank.cuh"
 
 namespace rwt {
 
@@ -119,52 +120,12 @@ __global__ void __launch_bounds__(256)
 // stage 2: one onesweep pass
 // ---------------------------------------------------------------------------
 
-template <int D, int THREADS>
-__device__ __forceinline__ void digit_exclusive_scan(const uint32_t* s_cnt,
-                                                     uint32_t* s_start,
-                                                     uint32_t* s_warp) {
-  constexpr int RADIX = 1 << D;
-  constexpr int R = (RADIX + THREADS - 1) / THREADS;  // digits per thread
-  static_assert(R * THREADS >= RADIX, "every digit needs a start offset");
-  const int first = threadIdx.x * R;
-  uint32_t local = 0;
-#pragma unroll
-  for (int r = 0; r < R; ++r) local += first + r < RADIX ? s_cnt[first + r] : 0u;
-  uint32_t total;
-  uint32_t run = block_exclusive_scan<THREADS>(local, s_warp, &total);
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    if (first + r < RADIX) {
-      s_start[first + r] = run;
-      run += s_cnt[first + r];
-    }
-  }
-}
 
 // Descriptors a look-back reads per round trip.
 constexpr int kLookback = 8;
 
-// Warp ranking schemes: all return, for each lane, the mask of valid lanes in
-// its warp holding the same digit (the lane's stable rank is the popcount of
-// the mask below it).
-enum RankMode : int { kRankBallot = 0, kRankMatchAny = 1, kRankAtomicOr = 2 };
-
-// D ballots, one per digit bit (warp-level multi-split).
-template <int D>
-__device__ __forceinline__ uint32_t match_ballot(uint32_t digit, uint32_t valid_mask) {
-  uint32_t peers = valid_mask;
-#pragma unroll
-  for (int b = 0; b < D; ++b) {
-    const bool bit = (digit >> b) & 1u;
-    const uint32_t v = __ballot_sync(0xffffffffu, bit);
-    peers &= bit ? v : ~v;
-  }
-  return peers;
-}
-
 template <typename K, int D, int THREADS, int KPT, int RANK>
 struct BinCfg {
-  static_assert(32 * KPT < 65536, "warp ranks are packed in 16 bits");
   static constexpr int RADIX = 1 << D;
   static constexpr int NW = THREADS / 32;
   static constexpr int TILE = THREADS * KPT;
@@ -175,63 +136,6 @@ struct BinCfg {
       kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
   static_assert(kSmem <= 227 * 1024, "onesweep variant exceeds shared memory per CTA");
 };
-
-// Stable ranks of one warp's 32*KPT keys among the warp's keys of the same
-// digit (order: step, then lane); the warp's digit counters `wh` advance.
-// FULL: every key is in range, so no per-key checks are made.
-template <int D, int KPT, int RANK, bool FULL, typename K>
-__device__ __forceinline__ void warp_rank(const K (&keys)[KPT], uint32_t (&rank2)[(KPT + 1) / 2],
-                                          int shift, uint32_t wbase, uint32_t n, uint32_t* wh,
-                                          uint32_t* wm) {
-  constexpr uint32_t RADIX = 1u << D;
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    const bool valid = FULL || wbase + 32u * i < n;
-    const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-    uint32_t peers;
-    if (RANK == kRankBallot) {
-      peers = match_ballot<D>(dig, FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid));
-    } else if (RANK == kRankMatchAny) {
-      peers = __match_any_sync(0xffffffffu, valid ? dig : 0xffffffffu);
-      if (!valid) peers = 0;
-    } else {
-      if (valid) atomicOr(&wm[dig], 1u << lane);
-      __syncwarp();
-      peers = valid ? wm[dig] : 0u;
-      __syncwarp();
-    }
-    const uint32_t below = __popc(peers & lanemask_lt());
-    uint32_t prev = 0;
-    if (valid && below == 0) {
-      // one shared-memory access for the read-modify-write of the counter
-      prev = atomicAdd(&wh[dig], uint32_t(__popc(peers)));
-      if (RANK == kRankAtomicOr) wm[dig] = 0;
-    }
-    const int leader = valid ? __ffs(peers) - 1 : int(lane);
-    prev = __shfl_sync(0xffffffffu, prev, leader);
-    const uint32_t r = prev + below;
-    if (i & 1) rank2[i >> 1] |= r << 16;
-    else rank2[i >> 1] = r;
-    __syncwarp();
-  }
-}
-
-// Places the warp's keys at their tile positions (wh: the warp's offsets).
-template <int D, int KPT, bool FULL, typename K>
-__device__ __forceinline__ void warp_place(const K (&keys)[KPT],
-                                           const uint32_t (&rank2)[(KPT + 1) / 2], int shift,
-                                           uint32_t wbase, uint32_t n, const uint32_t* wh,
-                                           K* s_keys) {
-  constexpr uint32_t RADIX = 1u << D;
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) {
-    if (FULL || wbase + 32u * i < n) {
-      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
-      s_keys[wh[dig] + ((rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu)] = keys[i];
-    }
-  }
-}
 
 // One onesweep pass over `n` keys: digit `shift`..`shift+D-1`, stable.
 // desc: [(tiles + 1) x RADIX] descriptors, row 0 prefilled with the global
@@ -273,7 +177,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
   // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
   K keys[KPT];
-  uint32_t rank2[(KPT + 1) / 2];  // warp ranks (< 32 * KPT), two per register
+  uint32_t rank2[RankPack<KPT>::kRegs];  // packed warp ranks
   const uint32_t wbase = base + warp * 32u * KPT + lane;
   uint32_t* wh = s_hist + warp * RADIX;
   uint32_t* wm = s_match + warp * RADIX;

@@ -4,7 +4,7 @@
 //  1. a stratified 64K-key sample of the input, sorted with the onesweep sort;
 //  2. 4,095 bucket boundaries.  Without the network boundary j is the sample
 //     key of rank c = 16(j+1) (the plain sample quantile).  With it, the MLP
-//     (mlp.cuh) reads a context of 16g sorted sample keys centred on c (eight
+//     (16 -> 64 -> 64 -> 1, BF16 weights, FP32 accumulation) reads a context of 16g sorted sample keys centred on c (eight
 //     inputs: mean positions of eight groups of 2g keys; eight more: the exact
 //     positions of the keys of ranks c-4 .. c+3; all normalised to the
 //     context's key range) and returns the boundary's offset from c in sample
@@ -12,13 +12,26 @@
 //     fractional rank.  This is a smoothed inversion of the sample's CDF that
 //     averages the sampling noise of the whole context instead of taking one
 //     order statistic.  A prefix maximum then makes the boundaries
-//     non-decreasing;//  3. bucket(k) = number of boundaries <= k, a non-decreasing function, so
-//     sorting every bucket and concatenating them sorts the input;
-//  4. one histogram pass, a plan (offsets, overflow), one scatter pass;
-//  5. one CTA per bucket sorts it in shared memory (stable LSD over only the
-//     bits its keys span); a bucket above the CTA's capacity is sorted by one
-//     CTA in chunks through global memory; a bucket above kBigCap sends the
-//     whole input back to the onesweep sort (decided on the host).
+//     non-decreasing;//  3. bucket(k) = number of boundaries <= k, found by descending a splitter
+//     tree; a non-decreasing function, so sorting every bucket and
+//     concatenating them sorts the input;
+//  4. two split passes, each writing runs long enough to coalesce: the
+//     first descends the top 8 levels of the splitter tree and scatters into
+//     256 super-bucket regions, the second descends each super-bucket's own
+//     4 levels into its 16 buckets.  Regions have fixed capacities (1.5x the
+//     mean super-bucket, 4x the mean bucket), so no histogram pass comes
+//     first; a tile counts its keys per bin, reserves each bin's run with one
+//     atomic and writes the run from shared memory.  The order inside a
+//     bucket is free (the bucket is sorted next);
+//  5. a plan (bucket offsets, overflow, big buckets first) and one CTA per
+//     bucket.  The output is keys only, so a bucket whose keys span at most
+//     2^15 values is a counting sort: a histogram over its value range,
+//     a scan, and an expansion of every value into its copies.  Wider buckets
+//     run a stable LSD in shared memory over the bits they span, with the
+//     onesweep passes' warp ranking; a bucket above one CTA's capacity is
+//     sorted by its CTA in chunks through global memory.  A region that
+//     overflowed sends the whole input to the onesweep sort (decided on the
+//     host, which reads the plan).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -28,7 +41,7 @@
 #include <vector>
 
 #include "internal.hpp"
-#include "mlp.cuh"
+#include "rank.cuh"
 
 namespace rwt {
 
@@ -37,14 +50,28 @@ constexpr uint32_t kSpacing = kSample / kBuckets;  // sample keys per bucket
 static_assert(kSpacing == uint32_t(kMlpIn), "one window of MLP inputs per bucket");
 constexpr int kBsThreads = 1024, kBsKpt = 32;
 constexpr uint32_t kBucketCap = kBsThreads * kBsKpt;  // keys one CTA sorts in smem
-constexpr uint32_t kBigCap = 1u << 21;              // beyond: onesweep for everything
-constexpr int kScThreads = 512, kScKpt = 32;
-constexpr uint32_t kScTile = kScThreads * kScKpt;
+
+// Region of one bucket for n keys: 4x the mean bucket size (at least the
+// mean + 64), a multiple of 32 keys.
+__host__ __device__ inline uint32_t region_cap(uint32_t n) {
+  const uint32_t mean = (n + kBuckets - 1) / kBuckets;
+  const uint32_t c = mean * 4 > mean + 64 ? mean * 4 : mean + 64;
+  return (c + 31) & ~31u;
+}
+
+constexpr uint32_t kSupers = 256;  // first split: top 8 tree levels
+constexpr uint32_t kCountSpan = 1u << 15;  // value range of the counting path
+
+// Region of one super-bucket for n keys: 1.5x the mean plus 1,024 keys.
+__host__ __device__ inline uint32_t super_cap(uint32_t n) {
+  const uint32_t mean = (n + kSupers - 1) / kSupers;
+  return (mean + mean / 2 + 1024 + 31) & ~31u;
+}
 
 struct LearnedPlan {
   uint32_t max_count;
   uint32_t n_big;       // buckets above kBucketCap
-  uint32_t fallback;    // some bucket above kBigCap
+  uint32_t fallback;    // some bucket overflowed its region
   uint32_t pad;
 };
 
@@ -71,78 +98,60 @@ __global__ void k_sample(const uint32_t* __restrict__ keys, uint32_t n,
 // Context group sizes the boundary MLP accepts (context = 16 * group keys).
 constexpr uint32_t kMaxGroup = 16;
 
-// MLP inputs of boundary j (sample rank c, context [c - half, c + half)).
+// MLP input i of boundary j (sample rank c, context [c - half, c + half)):
+// i < 8 the mean position of the i-th group of 2g context keys, i >= 8 the
+// position of the key of rank c - 12 + i; normalised to the context's range.
+__device__ __forceinline__ float boundary_feature(const uint32_t* __restrict__ s, uint32_t c,
+                                                  uint32_t half, uint32_t group, int i) {
+  const uint32_t* ctx = s + (c - half);
+  const uint32_t lo = ctx[0], span = max(ctx[2 * half - 1] - lo, 1u);
+  const float fspan = float(span);
+  if (i < kMlpIn / 2) {
+    const uint32_t g2 = 2 * group;  // keys per coarse group
+    uint64_t sum = 0;
+    for (uint32_t q = 0; q < g2; ++q) sum += ctx[i * g2 + q] - lo;
+    return __fdiv_rn(__ull2float_rn(sum), __fmul_rn(float(g2), fspan));
+  }
+  return __fdiv_rn(float(s[c - kMlpIn / 4 + (i - kMlpIn / 2)] - lo), fspan);
+}
+
 __device__ __forceinline__ void boundary_features(const uint32_t* __restrict__ s, uint32_t c,
                                                   uint32_t half, uint32_t group,
                                                   float (&x)[kMlpIn]) {
-  const uint32_t* ctx = s + (c - half);
-  const uint32_t lo = ctx[0], span = max(ctx[2 * half - 1] - lo, 1u);
-  const uint32_t g2 = 2 * group;  // keys per coarse group
-  const float fspan = float(span);
-  const float denom = __fmul_rn(float(g2), fspan);
 #pragma unroll
-  for (int i = 0; i < kMlpIn / 2; ++i) {
-    uint64_t sum = 0;
-    for (uint32_t q = 0; q < g2; ++q) sum += ctx[i * g2 + q] - lo;
-    x[i] = __fdiv_rn(__ull2float_rn(sum), denom);
-  }
-#pragma unroll
-  for (int i = 0; i < kMlpIn / 2; ++i)
-    x[kMlpIn / 2 + i] = __fdiv_rn(float(s[c - kMlpIn / 4 + i] - lo), fspan);
+  for (int i = 0; i < kMlpIn; ++i) x[i] = boundary_feature(s, c, half, group, i);
 }
 
-// 2. boundaries (and, for training, the MLP inputs of every boundary; rows
-// whose context does not fit inside the sample are written as zeros and keep
-// the sample quantile).  MLP boundaries still need k_bounds_monotone.
-template <bool USE_MLP>
+// Boundary key from the network's output y: offset d = y * half sample ranks
+// from c (clamped to the context), interpolated between the two sample keys
+// around the fractional rank c + d.
+__device__ __forceinline__ uint32_t boundary_from_output(const uint32_t* __restrict__ s,
+                                                         uint32_t c, uint32_t half, float y) {
+  const float fh = float(half);
+  const float d = fminf(fmaxf(__fmul_rn(y, fh), -fh), fh - 1.0f);
+  const float fl = floorf(d);
+  const uint32_t i0 = uint32_t(int(c) + int(fl));
+  const uint32_t i1 = min(i0 + 1, kSample - 1);
+  const uint32_t a0 = s[i0], gap = s[i1] - a0;
+  return a0 + min(uint32_t(__fmul_rn(d - fl, float(gap)) + 0.5f), gap);
+}
+
+// 2. sample-quantile boundaries (and, for training, the MLP inputs of every
+// boundary; rows whose context does not fit inside the sample are zero)
 __global__ void __launch_bounds__(256)
-    k_boundaries(const uint32_t* __restrict__ sorted_sample, const float* __restrict__ params,
-                 uint32_t group, uint32_t* __restrict__ bounds, float* __restrict__ features) {
-  __shared__ float s_w1[kMlpHidden * kMlpIn], s_w2[kMlpHidden * kMlpHidden], s_w3[kMlpHidden],
-      s_b1[kMlpHidden], s_b2[kMlpHidden];
-  if (USE_MLP) {
-    constexpr int oW1 = 0, oB1 = oW1 + kMlpHidden * kMlpIn, oW2 = oB1 + kMlpHidden,
-                  oB2 = oW2 + kMlpHidden * kMlpHidden, oW3 = oB2 + kMlpHidden;
-    for (int i = threadIdx.x; i < kMlpHidden * kMlpIn; i += blockDim.x)
-      s_w1[i] = __bfloat162float(__float2bfloat16_rn(params[oW1 + i]));
-    for (int i = threadIdx.x; i < kMlpHidden * kMlpHidden; i += blockDim.x)
-      s_w2[i] = __bfloat162float(__float2bfloat16_rn(params[oW2 + i]));
-    for (int i = threadIdx.x; i < kMlpHidden; i += blockDim.x) {
-      s_w3[i] = __bfloat162float(__float2bfloat16_rn(params[oW3 + i]));
-      s_b1[i] = params[oB1 + i];
-      s_b2[i] = params[oB2 + i];
-    }
-    __syncthreads();
-  }
+    k_boundaries(const uint32_t* __restrict__ sorted_sample, uint32_t group,
+                 uint32_t* __restrict__ bounds, float* __restrict__ features) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= kBounds) return;
   const uint32_t c = (j + 1) * kSpacing;  // sample rank of the ideal boundary
+  bounds[j] = sorted_sample[c];
+  if (!features) return;
   const uint32_t half = (kMlpIn / 2) * group;
   const bool fits = c >= half && c + half <= kSample;
-  uint32_t b = sorted_sample[c];
-  if ((USE_MLP || features) && fits) {
-    float x[kMlpIn];
-    boundary_features(sorted_sample, c, half, group, x);
-    if (features) {
+  float x[kMlpIn];
+  if (fits) boundary_features(sorted_sample, c, half, group, x);
 #pragma unroll
-      for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = x[i];
-    }
-    if (USE_MLP) {
-      // offset in sample ranks, d in [-half, half - 1]
-      const float y = mlp_eval(x, s_w1, s_b1, s_w2, s_b2, s_w3, params[kMlpParams - 1]);
-      const float fh = float(half);
-      const float d = fminf(fmaxf(__fmul_rn(y, fh), -fh), fh - 1.0f);
-      const float fl = floorf(d);
-      const uint32_t i0 = uint32_t(int(c) + int(fl));
-      const uint32_t i1 = min(i0 + 1, kSample - 1);
-      const uint32_t a0 = sorted_sample[i0], gap = sorted_sample[i1] - a0;
-      b = a0 + min(uint32_t(__fmul_rn(d - fl, float(gap)) + 0.5f), gap);
-    }
-  } else if (features) {
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = 0.0f;
-  }
-  bounds[j] = b;
+  for (int i = 0; i < kMlpIn; ++i) features[size_t(j) * kMlpIn + i] = fits ? x[i] : 0.0f;
 }
 
 // prefix maximum over the boundaries (one block): non-decreasing boundaries
@@ -211,250 +220,328 @@ __device__ __forceinline__ uint32_t bucket_of(const uint32_t* s_t, uint32_t k) {
   return i - kBuckets;
 }
 
-// 4a. histogram of the buckets
-__global__ void __launch_bounds__(512)
-    k_bucket_hist(const uint32_t* __restrict__ keys, uint32_t n,
-                  const uint32_t* __restrict__ bounds, uint32_t* __restrict__ counts) {
-  __shared__ uint32_t s_b[kBuckets], s_cnt[kBuckets];
-  load_tree(bounds, s_b);
-  for (int i = threadIdx.x; i < int(kBuckets); i += blockDim.x) s_cnt[i] = 0;
-  __syncthreads();
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    atomicAdd(&s_cnt[bucket_of(s_b, __ldcs(keys + i))], 1u);
-  __syncthreads();
-  for (int i = threadIdx.x; i < int(kBuckets); i += blockDim.x)
-    if (s_cnt[i]) atomicAdd(&counts[i], s_cnt[i]);
+// 2'. MLP boundaries, evaluated in parallel: 64 threads per boundary (one
+// hidden unit each), four boundaries per round, kBpRounds rounds per CTA.
+// The inputs are those k_boundaries writes for training.
+constexpr int kBpThreads = 256, kBpGroup = kBpThreads / kMlpHidden, kBpRounds = 1;
+constexpr uint32_t kBpPerCta = kBpGroup * kBpRounds;
+
+__global__ void __launch_bounds__(kBpThreads)
+    k_boundaries_mlp(const uint32_t* __restrict__ sorted_sample, const float* __restrict__ params,
+                     uint32_t group, uint32_t* __restrict__ bounds) {
+  __shared__ float s_w1[kMlpHidden * kMlpIn], s_w2[kMlpHidden * kMlpHidden], s_w3[kMlpHidden],
+      s_b1[kMlpHidden], s_b2[kMlpHidden];
+  __shared__ float s_x[kBpGroup][kMlpIn], s_h1[kBpGroup][kMlpHidden], s_part[kBpGroup][2];
+  constexpr int oW1 = 0, oB1 = oW1 + kMlpHidden * kMlpIn, oW2 = oB1 + kMlpHidden,
+                oB2 = oW2 + kMlpHidden * kMlpHidden, oW3 = oB2 + kMlpHidden;
+  for (int i = threadIdx.x; i < kMlpHidden * kMlpIn; i += kBpThreads)
+    s_w1[i] = __bfloat162float(__float2bfloat16_rn(params[oW1 + i]));
+  for (int i = threadIdx.x; i < kMlpHidden * kMlpHidden; i += kBpThreads)
+    s_w2[i] = __bfloat162float(__float2bfloat16_rn(params[oW2 + i]));
+  for (int i = threadIdx.x; i < kMlpHidden; i += kBpThreads) {
+    s_w3[i] = __bfloat162float(__float2bfloat16_rn(params[oW3 + i]));
+    s_b1[i] = params[oB1 + i];
+    s_b2[i] = params[oB2 + i];
+  }
+  const float b3 = params[kMlpParams - 1];
+  const int g = threadIdx.x / kMlpHidden, u = threadIdx.x % kMlpHidden;
+  const uint32_t half = (kMlpIn / 2) * group;
+  for (int r = 0; r < kBpRounds; ++r) {
+    const uint32_t j = (blockIdx.x * kBpRounds + r) * kBpGroup + g;
+    const uint32_t c = (j + 1) * kSpacing;
+    const bool live = j < kBounds;
+    const bool fits = live && c >= half && c + half <= kSample;
+    __syncthreads();  // weights loaded; the previous round's s_x / s_h1 read
+    if (fits && u < kMlpIn) s_x[g][u] = boundary_feature(sorted_sample, c, half, group, u);
+    __syncthreads();
+    if (fits) {
+      float acc = s_b1[u];
+#pragma unroll
+      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(s_w1[u * kMlpIn + k], s_x[g][k], acc);
+      s_h1[g][u] = fmaxf(acc, 0.0f);
+    }
+    __syncthreads();
+    float part = 0.0f;
+    if (fits) {
+      float acc = s_b2[u];
+#pragma unroll 16
+      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(s_w2[u * kMlpHidden + k], s_h1[g][k], acc);
+      part = s_w3[u] * fmaxf(acc, 0.0f);
+    }
+    part = warp_sum(part);
+    if ((threadIdx.x & 31) == 0) s_part[g][(threadIdx.x >> 5) & 1] = part;
+    __syncthreads();
+    if (u == 0 && live)
+      bounds[j] = fits ? boundary_from_output(sorted_sample, c, half,
+                                              b3 + s_part[g][0] + s_part[g][1])
+                       : sorted_sample[c];
+  }
 }
 
-// 4b. plan: offsets, write cursors, overflow summary (one block)
+// 4. one split pass.  Segment `seg` of the source (its keys: n, or
+// seg_counts[seg] at src + seg * src_cap) is split by the LEVELS tree levels
+// below node root0 + seg into 2^LEVELS bins; bin i goes to output region
+// out0 + i, out0 = (root0 + seg) * 2^LEVELS - 2^(depth of the bins' level).
+// Tiles of TILE keys: grid = segments * tiles_per_seg.
+constexpr int kSpThreads = 512, kSpKpt = 16;
+constexpr uint32_t kSpTile = kSpThreads * kSpKpt;
+
+template <int LEVELS>
+struct SplitCfg {
+  static constexpr uint32_t BINS = 1u << LEVELS;
+  static constexpr size_t kSmem = size_t(kSpTile) * 4 + size_t(kSpTile) + 4 * size_t(BINS) * 4;
+};
+
+template <int LEVELS>
+__global__ void __launch_bounds__(kSpThreads, 2)
+    k_split(const uint32_t* __restrict__ src, uint32_t n, const uint32_t* __restrict__ seg_counts,
+            uint32_t src_cap, uint32_t tiles_per_seg, uint32_t root0,
+            const uint32_t* __restrict__ bounds, uint32_t* __restrict__ cursor,
+            uint32_t* __restrict__ region, uint32_t cap) {
+  using C = SplitCfg<LEVELS>;
+  constexpr uint32_t BINS = C::BINS;
+  static_assert(BINS <= 256, "bins are kept in bytes");
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint32_t* s_keys = sm;                                   // [kSpTile]
+  uint8_t* s_bin = reinterpret_cast<uint8_t*>(s_keys + kSpTile);  // [kSpTile]
+  uint32_t* s_t = reinterpret_cast<uint32_t*>(s_bin + kSpTile);   // local tree [BINS]
+  uint32_t* s_cnt = s_t + BINS;
+  uint32_t* s_start = s_cnt + BINS;
+  uint32_t* s_base = s_start + BINS;
+  const uint32_t seg = blockIdx.x / tiles_per_seg, chunk = blockIdx.x % tiles_per_seg;
+  const uint32_t seg_n = seg_counts ? min(seg_counts[seg], src_cap) : n;
+  const uint32_t base = chunk * kSpTile;
+  if (base >= seg_n) return;  // the whole CTA: the segment is shorter
+  const uint32_t* in = src + size_t(seg) * src_cap + base;
+  const uint32_t tile_n = min(kSpTile, seg_n - base);
+  const uint32_t root = root0 + seg;
+  const int root_depth = 31 - __clz(root);
+  // the subtree below root, LEVELS deep, as a local heap (local node m at
+  // depth d = global node root * 2^d + m - 2^d)
+  for (uint32_t m = threadIdx.x + 1; m < BINS; m += kSpThreads) {
+    const int d = 31 - __clz(m);
+    const uint32_t g = (root << d) + (m - (1u << d));
+    const int D = root_depth + d;
+    const uint32_t pg = g - (1u << D);
+    s_t[m] = bounds[((2 * pg + 1) << (11 - D)) - 1];
+  }
+  for (uint32_t i = threadIdx.x; i < BINS; i += kSpThreads) s_cnt[i] = 0;
+  __syncthreads();
+  uint32_t k[kSpKpt];
+  const bool full = tile_n == kSpTile;
+  if (full) {
+    const uint4* v = reinterpret_cast<const uint4*>(in);
+#pragma unroll
+    for (int i = 0; i < kSpKpt / 4; ++i) {
+      const uint4 q = __ldcs(v + threadIdx.x + i * kSpThreads);
+      k[4 * i] = q.x;
+      k[4 * i + 1] = q.y;
+      k[4 * i + 2] = q.z;
+      k[4 * i + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kSpKpt / 4; ++i)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t p = 4 * (threadIdx.x + i * kSpThreads) + e;
+        k[4 * i + e] = p < tile_n ? in[p] : 0u;
+      }
+  }
+  // bins, 8 keys at a time level by level; the count atomic's old value is
+  // the key's slot in its bin's run (any order inside a bucket will do)
+  uint32_t meta[kSpKpt];  // bin | slot << 8
+#pragma unroll
+  for (int i0 = 0; i0 < kSpKpt; i0 += 8) {
+    uint32_t m[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) m[j] = 1;
+#pragma unroll
+    for (int lvl = 0; lvl < LEVELS; ++lvl)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) m[j] = 2 * m[j] + (k[i0 + j] >= s_t[m[j]] ? 1u : 0u);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int i = i0 + j;
+      const uint32_t p = 4 * (threadIdx.x + (i / 4) * kSpThreads) + (i % 4);
+      const uint32_t bin = m[j] - BINS;
+      meta[i] = p < tile_n ? bin | (atomicAdd(&s_cnt[bin], 1u) << 8) : 0xffffffffu;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan of the bin counts (BINS <= 256)
+    uint32_t run = 0;
+    for (uint32_t b0 = 0; b0 < BINS; b0 += 32) {
+      const uint32_t c = b0 + threadIdx.x < BINS ? s_cnt[b0 + threadIdx.x] : 0u;
+      const uint32_t inc = warp_inclusive_scan(c);
+      if (b0 + threadIdx.x < BINS) s_start[b0 + threadIdx.x] = run + inc - c;
+      run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+  }
+  const uint32_t out0 = (root << LEVELS) - (1u << (root_depth + LEVELS));
+  for (uint32_t b = threadIdx.x; b < BINS; b += kSpThreads) {
+    const uint32_t c = s_cnt[b];
+    s_base[b] = c ? atomicAdd(&cursor[out0 + b], c) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kSpKpt; ++i) {
+    if (meta[i] != 0xffffffffu) {
+      const uint32_t bin = meta[i] & 0xffu, q = s_start[bin] + (meta[i] >> 8);
+      s_keys[q] = k[i];
+      s_bin[q] = uint8_t(bin);
+    }
+  }
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < tile_n; q += kSpThreads) {
+    const uint32_t bin = s_bin[q];
+    const uint32_t pos = s_base[bin] + (q - s_start[bin]);
+    if (pos < cap) region[size_t(out0 + bin) * cap + pos] = s_keys[q];
+  }
+}
+
+// 5a. plan (one block): bucket offsets, overflow, and the order the bucket
+// sort takes the buckets in: those above one CTA's capacity first (they take
+// longest), the rest after them.
 __global__ void __launch_bounds__(1024)
-    k_bucket_plan(const uint32_t* __restrict__ counts, uint32_t* __restrict__ offsets,
-                  uint32_t* __restrict__ cursor, LearnedPlan* __restrict__ plan) {
+    k_bucket_plan(const uint32_t* __restrict__ counts, uint32_t cap,
+                  const uint32_t* __restrict__ super_counts, uint32_t scap,
+                  uint32_t* __restrict__ offsets, uint32_t* __restrict__ order,
+                  LearnedPlan* __restrict__ plan) {
   __shared__ uint32_t s_warp[33];
+  __shared__ uint32_t s_front, s_back;
   constexpr int R = kBuckets / 1024;
+  if (threadIdx.x == 0) s_front = s_back = 0;
   const int first = threadIdx.x * R;
-  uint32_t v[R], local = 0, mx = 0, big = 0;
+  uint32_t v[R], local = 0, mx = 0, big = 0, over = 0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     v[r] = counts[first + r];
     local += v[r];
     mx = max(mx, v[r]);
-    big += v[r] > kBucketCap;
+    big += v[r] > kBucketCap && v[r] <= cap;
+    over |= v[r] > cap;
   }
+  if (threadIdx.x < kSupers) over |= super_counts[threadIdx.x] > scap;
   uint32_t total;
-  uint32_t run = block_exclusive_scan<1024>(local, s_warp, &total);
+  uint32_t run = block_exclusive_scan<1024>(local, s_warp, &total);  // synchronises
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     offsets[first + r] = run;
-    cursor[first + r] = run;
     run += v[r];
+    if (v[r] > kBucketCap) order[atomicAdd(&s_front, 1u)] = first + r;
+    else order[kBuckets - 1 - atomicAdd(&s_back, 1u)] = first + r;
   }
-  offsets[kBuckets] = total;
+  if (threadIdx.x == 0) offsets[kBuckets] = total;
   atomicMax(&plan->max_count, mx);
   if (big) atomicAdd(&plan->n_big, big);
-  if (mx > kBigCap) plan->fallback = 1;
+  if (over) plan->fallback = 1;
 }
 
-// 4c. scatter into the buckets: within a tile keys are grouped by bucket in
-// shared memory and each bucket's run is written at a position reserved with
-// one atomic on the bucket's cursor (the order inside a bucket is free: the
-// bucket is sorted next).  The bucket id of every placed key is kept in shared
-// memory so that the write-out does not search the boundaries again.
-__global__ void __launch_bounds__(kScThreads)
-    k_bucket_scatter(const uint32_t* __restrict__ keys, uint32_t n,
-                     const uint32_t* __restrict__ bounds, uint32_t* __restrict__ cursor,
-                     uint32_t* __restrict__ out) {
-  extern __shared__ __align__(16) uint32_t sm[];
-  uint32_t* s_keys = sm;                  // [kScTile]
-  uint32_t* s_b = s_keys + kScTile;       // [kBuckets] splitter tree
-  uint32_t* s_cnt = s_b + kBuckets;       // [kBuckets] counts, then global bases
-  uint32_t* s_pos = s_cnt + kBuckets;     // [kBuckets] starts, then fill cursors
-  uint32_t* s_start = s_pos + kBuckets;   // [kBuckets]
-  uint16_t* s_bid = reinterpret_cast<uint16_t*>(s_start + kBuckets);  // [kScTile]
-  uint32_t* s_warp = reinterpret_cast<uint32_t*>(s_bid + kScTile);    // [kScThreads/32+1]
-  load_tree(bounds, s_b);
-  for (int i = threadIdx.x; i < int(kBuckets); i += kScThreads) s_cnt[i] = 0;
-  __syncthreads();
-  const uint32_t base = blockIdx.x * kScTile;
-  uint32_t k[kScKpt];
-  uint16_t bid[kScKpt];
-#pragma unroll
-  for (int i = 0; i < kScKpt; ++i) {
-    const uint32_t idx = base + i * kScThreads + threadIdx.x;
-    k[i] = idx < n ? __ldcs(keys + idx) : 0u;
-    bid[i] = uint16_t(bucket_of(s_b, k[i]));
-    if (idx < n) atomicAdd(&s_cnt[bid[i]], 1u);
-  }
-  __syncthreads();
-  constexpr int R = kBuckets / kScThreads;
-  const int first = threadIdx.x * R;
-  uint32_t c[R], local = 0;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    c[r] = s_cnt[first + r];
-    local += c[r];
-  }
-  uint32_t total;
-  uint32_t run = block_exclusive_scan<kScThreads>(local, s_warp, &total);
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    s_start[first + r] = run;
-    s_pos[first + r] = run;
-    run += c[r];
-    s_cnt[first + r] = c[r] ? atomicAdd(&cursor[first + r], c[r]) : 0u;  // global base
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < kScKpt; ++i) {
-    const uint32_t idx = base + i * kScThreads + threadIdx.x;
-    if (idx < n) {
-      const uint32_t p = atomicAdd(&s_pos[bid[i]], 1u);
-      s_keys[p] = k[i];
-      s_bid[p] = bid[i];
-    }
-  }
-  __syncthreads();
-  const uint32_t tile_n = min(kScTile, n - base);
-  for (uint32_t p = threadIdx.x; p < tile_n; p += kScThreads) {
-    const uint32_t b = s_bid[p];
-    out[s_cnt[b] + (p - s_start[b])] = s_keys[p];
-  }
-}
+// smem of the bucket sort: keys, per-warp counters and match masks, digit
+// totals and starts, scan scratch
+constexpr int kBsWarps = kBsThreads / 32;
+constexpr size_t kBsSmem = (size_t(kBucketCap) + 2 * size_t(kBsWarps) * 256 + 2 * 256 + 64) * 4;
 
-constexpr size_t kScSmem =
-    (size_t(kScTile) + 4 * size_t(kBuckets) + 64) * 4 + size_t(kScTile) * 2;
-
-// Stable block-wide LSD sort of `cnt` <= kBucketCap keys held in registers
-// (warp w holds items [w*32*KPT, (w+1)*32*KPT), step i, lane l -> item
-// w*32*KPT + i*32 + l), over bits [0, bits).  Each pass counts the digits per
-// warp (shared-memory atomic-OR peer matching), scans them, then ranks again
-// and scatters straight to shared memory: no ranks are kept in registers.
-// The result is left in s_keys[0, cnt).
-template <int THREADS, int KPT>
-__device__ void block_lsd_sort(uint32_t (&k)[KPT], uint32_t cnt, int bits, uint32_t* s_keys,
-                               uint32_t* s_hist, uint32_t* s_match, uint32_t* s_tot,
-                               uint32_t* s_warp) {
-  constexpr int NW = THREADS / 32, RADIX = 256;
+// Counting sort of a bucket whose keys lie in [lo, lo + span), span <= 2^15:
+// the sorted keys are fixed by how often each value occurs.  Histogram in
+// shared memory (over the key buffer), exclusive scan, then every value is
+// written as its run of copies: runs of up to 32 by the thread that owns the
+// value, longer runs by a whole warp from a queue.
+template <int KPT>
+__device__ void bucket_count_sort(const uint32_t (&k)[KPT], int steps, uint32_t wbase,
+                                  uint32_t wend, uint32_t lo, uint32_t span, uint32_t cnt,
+                                  uint32_t* __restrict__ dst, uint32_t* sm) {
+  uint32_t* s_c = sm;                   // [span] counts, then run starts
+  uint32_t* s_q = sm + kBucketCap;      // queue of long runs: (value, start, length)
+  uint32_t* s_misc = s_q + 3 * 1024;    // [0] queue length, [8..41] warp totals
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  const uint32_t wbase = warp * 32u * KPT + lane;
-  uint32_t* wh = s_hist + warp * RADIX;
-  uint32_t* wm = s_match + warp * RADIX;
-  for (int shift = 0; shift < bits; shift += 8) {
-    for (int i = threadIdx.x; i < NW * RADIX; i += THREADS) {
-      s_hist[i] = 0;
-      s_match[i] = 0;
-    }
-    __syncthreads();
-    // count per warp
+  const uint32_t span4 = (span + 3) & ~3u;
+  for (uint32_t i = threadIdx.x; i < span4 / 4; i += kBsThreads)
+    reinterpret_cast<uint4*>(s_c)[i] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) s_misc[0] = 0;
+  __syncthreads();
 #pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const bool valid = wbase + 32u * i < cnt;
-      const uint32_t dig = (k[i] >> shift) & 255u;
-      if (valid) atomicOr(&wm[dig], 1u << lane);
-      __syncwarp();
-      const uint32_t peers = valid ? wm[dig] : 0u;
-      __syncwarp();
-      if (valid && __popc(peers & lanemask_lt()) == 0) {
-        wh[dig] += __popc(peers);
-        wm[dig] = 0;
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-    // digit totals, exclusive over digits, then per-warp starts
-    if (threadIdx.x < RADIX) {
-      uint32_t t = 0;
-      for (int w = 0; w < NW; ++w) t += s_hist[w * RADIX + threadIdx.x];
-      s_tot[threadIdx.x] = t;
-    }
-    __syncthreads();
-    {
-      const uint32_t t = threadIdx.x < RADIX ? s_tot[threadIdx.x] : 0u;
-      uint32_t tot;
-      const uint32_t ex = block_exclusive_scan<THREADS>(t, s_warp, &tot);
-      if (threadIdx.x < RADIX) {
-        uint32_t run = ex;
-        for (int w = 0; w < NW; ++w) {
-          const uint32_t c = s_hist[w * RADIX + threadIdx.x];
-          s_hist[w * RADIX + threadIdx.x] = run;
-          run += c;
-        }
-      }
-    }
-    __syncthreads();
-    // rank again and scatter
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const bool valid = wbase + 32u * i < cnt;
-      const uint32_t dig = (k[i] >> shift) & 255u;
-      if (valid) atomicOr(&wm[dig], 1u << lane);
-      __syncwarp();
-      const uint32_t peers = valid ? wm[dig] : 0u;
-      __syncwarp();
-      const uint32_t below = __popc(peers & lanemask_lt());
-      uint32_t prev = 0;
-      if (valid && below == 0) {
-        prev = wh[dig];
-        wh[dig] = prev + __popc(peers);
-        wm[dig] = 0;
-      }
-      const int leader = valid ? __ffs(peers) - 1 : int(lane);
-      prev = __shfl_sync(0xffffffffu, prev, leader);
-      if (valid) s_keys[prev + below] = k[i];
-      __syncwarp();
-    }
-    __syncthreads();
-    if (shift + 8 < bits) {
-#pragma unroll
-      for (int i = 0; i < KPT; ++i) {
-        const uint32_t idx = wbase + 32u * i;
-        k[i] = idx < cnt ? s_keys[idx] : 0u;
-      }
-      __syncthreads();
+  for (int i = 0; i < KPT; ++i)
+    if (i < steps && wbase + 32u * i < wend) atomicAdd(&s_c[k[i] - lo], 1u);
+  __syncthreads();
+  // exclusive scan of s_c[0, span): warp w scans the counters
+  // [w*per, (w+1)*per) 32 at a time, after the totals of the earlier warps
+  const uint32_t per = ((span + kBsWarps - 1) / kBsWarps + 31) & ~31u;
+  const uint32_t w0 = min(span, warp * per), w1 = min(span, w0 + per);
+  uint32_t tot = 0;
+  for (uint32_t i = w0 + lane; i < w1; i += 32) tot += s_c[i];
+  tot = warp_sum(tot);
+  if (lane == 0) s_misc[8 + warp] = tot;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = s_misc[8 + lane];
+    const uint32_t inc = warp_inclusive_scan(t);
+    s_misc[8 + lane] = inc - t;
+  }
+  __syncthreads();
+  uint32_t run = s_misc[8 + warp];
+  for (uint32_t b0 = w0; b0 < w1; b0 += 32) {
+    const uint32_t i = b0 + lane;
+    const uint32_t c = i < w1 ? s_c[i] : 0u;
+    const uint32_t inc = warp_inclusive_scan(c);
+    if (i < w1) s_c[i] = run + inc - c;
+    run += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  __syncthreads();
+  // expansion
+  for (uint32_t v = threadIdx.x; v < span; v += kBsThreads) {
+    const uint32_t o = s_c[v], e = v + 1 < span ? s_c[v + 1] : cnt;
+    const uint32_t c = e - o;
+    if (c > 32) {
+      const uint32_t qi = atomicAdd(&s_misc[0], 1u);
+      s_q[3 * qi] = lo + v;
+      s_q[3 * qi + 1] = o;
+      s_q[3 * qi + 2] = c;
+    } else {
+      for (uint32_t j = 0; j < c; ++j) dst[o + j] = lo + v;
     }
   }
-  if (bits <= 0) {  // every key equal: keep them as they are
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const uint32_t idx = wbase + 32u * i;
-      if (idx < cnt) s_keys[idx] = k[i];
-    }
-    __syncthreads();
+  __syncthreads();
+  const uint32_t nq = s_misc[0];
+  for (uint32_t qi = warp; qi < nq; qi += kBsWarps) {
+    const uint32_t val = s_q[3 * qi], o = s_q[3 * qi + 1], c = s_q[3 * qi + 2];
+    for (uint32_t j = lane; j < c; j += 32) dst[o + j] = val;
   }
 }
 
-// smem layout of the bucket sort kernel
-constexpr size_t kBsSmem =
-    (size_t(kBucketCap) + 2 * size_t(kBsThreads / 32) * 256 + 256 + 64) * 4;
-
-// 5a. one CTA per bucket of at most kBucketCap keys
-__global__ void __launch_bounds__(kBsThreads, 1)
-    k_bucket_sort(const uint32_t* __restrict__ in, const uint32_t* __restrict__ offsets,
-                  uint32_t* __restrict__ out) {
-  extern __shared__ __align__(16) uint32_t sm[];
+// A bucket of up to kBucketCap keys: keys in registers (warp w owns
+// [w*32*KPT, (w+1)*32*KPT)), one stable LSD pass per 8 spanned bits with the
+// onesweep ranking (warp_rank / warp_place), ending in s_keys.
+__device__ void bucket_sort_small(const uint32_t* __restrict__ src, uint32_t cnt,
+                                  uint32_t* __restrict__ dst, uint32_t* sm) {
+  constexpr int KPT = kBsKpt, RADIX = 256;
   uint32_t* s_keys = sm;
   uint32_t* s_hist = s_keys + kBucketCap;
-  uint32_t* s_match = s_hist + (kBsThreads / 32) * 256;
-  uint32_t* s_tot = s_match + (kBsThreads / 32) * 256;
-  uint32_t* s_warp = s_tot + 256;
-  const uint32_t b = blockIdx.x;
-  const uint32_t off = offsets[b], cnt = offsets[b + 1] - off;
-  if (cnt == 0 || cnt > kBucketCap) return;
+  uint32_t* s_match = s_hist + kBsWarps * RADIX;
+  uint32_t* s_cnt = s_match + kBsWarps * RADIX;
+  uint32_t* s_start = s_cnt + RADIX;
+  uint32_t* s_warp = s_start + RADIX;
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  const uint32_t wbase = warp * 32u * kBsKpt + lane;
-  uint32_t k[kBsKpt];
+  // the bucket spread evenly over the warps: warp w holds [w*per, (w+1)*per)
+  // (per a multiple of 32), so every warp runs only `steps` of its KPT steps
+  const uint32_t per = ((cnt + kBsWarps - 1) / kBsWarps + 31) & ~31u;
+  const int steps = int(per / 32);
+  const uint32_t wbase = warp * per + lane;
+  const uint32_t wend = min(cnt, (warp + 1) * per);  // end of this warp's keys
+  uint32_t k[KPT];
   uint32_t mn = 0xffffffffu, mx = 0;
 #pragma unroll
-  for (int i = 0; i < kBsKpt; ++i) {
+  for (int i = 0; i < KPT; ++i) {
     const uint32_t idx = wbase + 32u * i;
-    k[i] = idx < cnt ? in[off + idx] : 0u;
-    if (idx < cnt) {
+    const bool v = i < steps && idx < wend;
+    k[i] = v ? src[idx] : 0u;
+    if (v) {
       mn = min(mn, k[i]);
       mx = max(mx, k[i]);
     }
   }
-  // key span of the bucket: only the bits below the common prefix are sorted
+  // bits the bucket spans: only those below the common prefix are sorted
   for (int d = 16; d > 0; d >>= 1) {
     mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
     mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
@@ -469,38 +556,74 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     atomicMax(&s_warp[41], mx);
   }
   __syncthreads();
-  const uint32_t diff = s_warp[40] ^ s_warp[41];
+  const uint32_t lo = s_warp[40], hi = s_warp[41];
+  const uint32_t diff = lo ^ hi;
   const int bits = diff ? 32 - __clz(diff) : 0;
-  __syncthreads();
-  block_lsd_sort<kBsThreads, kBsKpt>(k, cnt, bits, s_keys, s_hist, s_match, s_tot, s_warp);
-  for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads) out[off + p] = s_keys[p];
+  if (bits != 0 && hi - lo < kCountSpan) {
+    bucket_count_sort(k, steps, wbase, wend, lo, hi - lo + 1, cnt, dst, sm);
+    return;
+  }
+  if (bits == 0) {  // every key equal
+#pragma unroll
+    for (int i = 0; i < KPT; ++i)
+      if (i < steps && wbase + 32u * i < wend) dst[wbase + 32u * i] = k[i];
+    return;
+  }
+  uint32_t* wh = s_hist + warp * RADIX;
+  uint32_t* wm = s_match + warp * RADIX;
+  uint32_t rank2[RankPack<KPT>::kRegs];
+  for (int shift = 0; shift < bits; shift += 8) {
+    {
+      const uint4 z = make_uint4(0, 0, 0, 0);
+      for (int i = threadIdx.x; i < 2 * kBsWarps * RADIX / 4; i += kBsThreads)
+        reinterpret_cast<uint4*>(s_hist)[i] = z;
+    }
+    __syncthreads();
+    warp_rank<8, KPT, kRankAtomicOr, false>(k, rank2, shift, wbase, wend, wh, wm, steps);
+    __syncthreads();
+    if (threadIdx.x < RADIX) {
+      uint32_t run = 0;
+      for (int w = 0; w < kBsWarps; ++w) {
+        const uint32_t c = s_hist[w * RADIX + threadIdx.x];
+        s_hist[w * RADIX + threadIdx.x] = run;
+        run += c;
+      }
+      s_cnt[threadIdx.x] = run;
+    }
+    __syncthreads();
+    digit_exclusive_scan<8, kBsThreads>(s_cnt, s_start, s_warp);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBsWarps * RADIX; i += kBsThreads)
+      s_hist[i] += s_start[i & (RADIX - 1)];
+    __syncthreads();
+    warp_place<8, KPT, false>(k, rank2, shift, wbase, wend, wh, s_keys, steps);
+    __syncthreads();
+    if (shift + 8 < bits) {
+#pragma unroll
+      for (int i = 0; i < KPT; ++i) {
+        const uint32_t idx = wbase + 32u * i;
+        k[i] = i < steps && idx < wend ? s_keys[idx] : 0u;
+      }
+    }
+  }
+  for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads) dst[p] = s_keys[p];
 }
 
-// 5b. a bucket above kBucketCap, one CTA, LSD through global memory: every
-// pass histograms the whole bucket, then places chunks of kBucketCap keys in
-// order (stable), ping-ponging between the bucket's ranges in `a` and `b`.
-// The sorted bucket ends in `out` (== a or b).
-__global__ void __launch_bounds__(kBsThreads, 1)
-    k_bucket_sort_big(uint32_t* __restrict__ a, uint32_t* __restrict__ bb,
-                      const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ counts,
-                      uint32_t* __restrict__ out) {
-  extern __shared__ __align__(16) uint32_t sm[];
-  uint32_t* s_keys = sm;
-  uint32_t* s_hist = s_keys + kBucketCap;
-  uint32_t* s_match = s_hist + (kBsThreads / 32) * 256;
-  uint32_t* s_tot = s_match + (kBsThreads / 32) * 256;
-  uint32_t* s_warp = s_tot + 256;
-  const uint32_t bkt = blockIdx.x;
-  const uint32_t off = offsets[bkt], cnt = counts[bkt];
-  if (cnt <= kBucketCap || cnt > kBigCap) return;
-  constexpr int NW = kBsThreads / 32, RADIX = 256;
+// A bucket above kBucketCap: stable LSD through global memory, ping-ponging
+// between the bucket's region `a` and its output range `b`; every pass
+// histograms the bucket, then places chunks of kBucketCap keys in order.
+__device__ __noinline__ void bucket_sort_big(uint32_t* __restrict__ a, uint32_t cnt, uint32_t* __restrict__ b,
+                                uint32_t* sm) {
+  constexpr int KPT = kBsKpt, RADIX = 256;
+  uint32_t* s_hist = sm + kBucketCap;
+  uint32_t* s_match = s_hist + kBsWarps * RADIX;
+  uint32_t* s_run = s_match + kBsWarps * RADIX;  // running digit starts across chunks
+  uint32_t* s_warp = s_run + 2 * RADIX;
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  // key span
   uint32_t mn = 0xffffffffu, mx = 0;
   for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads) {
-    const uint32_t v = a[off + p];
-    mn = min(mn, v);
-    mx = max(mx, v);
+    mn = min(mn, a[p]);
+    mx = max(mx, a[p]);
   }
   if (threadIdx.x == 0) {
     s_warp[40] = 0xffffffffu;
@@ -512,12 +635,11 @@ __global__ void __launch_bounds__(kBsThreads, 1)
   __syncthreads();
   const uint32_t diff = s_warp[40] ^ s_warp[41];
   const int bits = diff ? 32 - __clz(diff) : 0;
-  __syncthreads();
-  uint32_t* src = a + off;
-  uint32_t* dst = bb + off;
-  uint32_t* s_run = s_tot;  // running digit starts across chunks
+  uint32_t* src = a;
+  uint32_t* dst = b;
+  uint32_t* wh = s_hist + warp * RADIX;
+  uint32_t* wm = s_match + warp * RADIX;
   for (int shift = 0; shift < bits; shift += 8) {
-    // digit histogram of the whole bucket -> exclusive starts
     for (int i = threadIdx.x; i < RADIX; i += kBsThreads) s_hist[i] = 0;
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads)
@@ -532,40 +654,26 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     __syncthreads();
     for (uint32_t c0 = 0; c0 < cnt; c0 += kBucketCap) {
       const uint32_t ccount = min(kBucketCap, cnt - c0);
-      const uint32_t wbase = warp * 32u * kBsKpt + lane;
-      uint32_t k[kBsKpt];
+      const uint32_t wbase = warp * 32u * KPT + lane;
+      uint32_t k[KPT];
+      uint32_t rank2[RankPack<KPT>::kRegs];
 #pragma unroll
-      for (int i = 0; i < kBsKpt; ++i) {
+      for (int i = 0; i < KPT; ++i) {
         const uint32_t idx = wbase + 32u * i;
         k[i] = idx < ccount ? src[c0 + idx] : 0u;
       }
-      // per-warp counts of this chunk
-      uint32_t* wh = s_hist + warp * RADIX;
-      uint32_t* wm = s_match + warp * RADIX;
-      for (int i = threadIdx.x; i < NW * RADIX; i += kBsThreads) {
-        s_hist[i] = 0;
-        s_match[i] = 0;
+      {
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        for (int i = threadIdx.x; i < 2 * kBsWarps * RADIX / 4; i += kBsThreads)
+          reinterpret_cast<uint4*>(s_hist)[i] = z;
       }
       __syncthreads();
-#pragma unroll
-      for (int i = 0; i < kBsKpt; ++i) {
-        const bool valid = wbase + 32u * i < ccount;
-        const uint32_t dig = (k[i] >> shift) & 255u;
-        if (valid) atomicOr(&wm[dig], 1u << lane);
-        __syncwarp();
-        const uint32_t peers = valid ? wm[dig] : 0u;
-        __syncwarp();
-        if (valid && __popc(peers & lanemask_lt()) == 0) {
-          wh[dig] += __popc(peers);
-          wm[dig] = 0;
-        }
-        __syncwarp();
-      }
+      warp_rank<8, KPT, kRankAtomicOr, false>(k, rank2, shift, wbase, ccount, wh, wm);
       __syncthreads();
       // per-warp starts = running start of the digit + earlier warps
       if (threadIdx.x < RADIX) {
         uint32_t run = s_run[threadIdx.x];
-        for (int w = 0; w < NW; ++w) {
+        for (int w = 0; w < kBsWarps; ++w) {
           const uint32_t c = s_hist[w * RADIX + threadIdx.x];
           s_hist[w * RADIX + threadIdx.x] = run;
           run += c;
@@ -574,24 +682,11 @@ __global__ void __launch_bounds__(kBsThreads, 1)
       }
       __syncthreads();
 #pragma unroll
-      for (int i = 0; i < kBsKpt; ++i) {
-        const bool valid = wbase + 32u * i < ccount;
-        const uint32_t dig = (k[i] >> shift) & 255u;
-        if (valid) atomicOr(&wm[dig], 1u << lane);
-        __syncwarp();
-        const uint32_t peers = valid ? wm[dig] : 0u;
-        __syncwarp();
-        const uint32_t below = __popc(peers & lanemask_lt());
-        uint32_t prev = 0;
-        if (valid && below == 0) {
-          prev = wh[dig];
-          wh[dig] = prev + __popc(peers);
-          wm[dig] = 0;
+      for (int i = 0; i < KPT; ++i) {
+        if (wbase + 32u * i < ccount) {
+          const uint32_t pos = wh[(k[i] >> shift) & 255u] + RankPack<KPT>::get(rank2, i);
+          if (pos < cnt) dst[pos] = k[i];
         }
-        const int leader = valid ? __ffs(peers) - 1 : int(lane);
-        prev = __shfl_sync(0xffffffffu, prev, leader);
-        if (valid && prev + below < cnt) dst[prev + below] = k[i];
-        __syncwarp();
       }
       __syncthreads();
     }
@@ -601,8 +696,23 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     __threadfence_block();
     __syncthreads();
   }
-  if (src != out + off)
-    for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads) out[off + p] = src[p];
+  if (src != b)
+    for (uint32_t p = threadIdx.x; p < cnt; p += kBsThreads) b[p] = src[p];
+}
+
+// 5b. one CTA per bucket, in plan order
+__global__ void __launch_bounds__(kBsThreads, 1)
+    k_bucket_sort(uint32_t* __restrict__ region, uint32_t cap, const uint32_t* __restrict__ counts,
+                  const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ order,
+                  uint32_t* __restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  const uint32_t bk = order[blockIdx.x];
+  const uint32_t cnt = counts[bk];
+  if (cnt == 0 || cnt > cap) return;
+  uint32_t* src = region + size_t(bk) * cap;
+  uint32_t* dst = out + offsets[bk];
+  if (cnt > kBucketCap) bucket_sort_big(src, cnt, dst, sm);
+  else bucket_sort_small(src, cnt, dst, sm);
 }
 
 }  // namespace rwt
@@ -613,12 +723,14 @@ __global__ void __launch_bounds__(kBsThreads, 1)
 
 struct rw_tree_learned {
   uint32_t n_max = 0;
+  uint32_t cap_max = 0;   // bucket region capacity for n_max keys
+  uint32_t scap_max = 0;  // super-bucket region capacity for n_max keys
   int num_sms = 148;
   rw_tree_im_storage* sample_im = nullptr;  // onesweep scratch for the sample
   void* d_mem = nullptr;
   uint32_t *d_sample = nullptr, *d_sample_sorted = nullptr, *d_bounds = nullptr,
-           *d_counts = nullptr, *d_offsets = nullptr, *d_cursor = nullptr,
-           *d_tmp = nullptr;
+           *d_cursor = nullptr, *d_offsets = nullptr, *d_order = nullptr, *d_region = nullptr,
+           *d_super_cursor = nullptr, *d_super_region = nullptr;
   float* d_params = nullptr;
   float* d_features = nullptr;
   rwt::LearnedPlan* d_plan = nullptr;
@@ -651,16 +763,22 @@ int sort_sample(rw_tree_learned* L, cudaStream_t s) {
 
 int boundaries(rw_tree_learned* L, bool mlp, bool features, cudaStream_t s) {
   if (mlp && !L->has_params) return RW_ERR_NOT_READY;
-  float* f = features ? L->d_features : nullptr;
   const uint32_t blocks = (rwt::kBounds + 255) / 256;
+  if (features) {  // training data (the per-boundary kernel writes the inputs)
+    rwt::k_boundaries<<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->group, L->d_bounds,
+                                             L->d_features);
+    RWL_CUDA(cudaGetLastError());
+  }
   if (mlp) {
-    rwt::k_boundaries<true><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params, L->group,
-                                                   L->d_bounds, f);
+    const uint32_t ctas = (rwt::kBounds + rwt::kBpPerCta - 1) / rwt::kBpPerCta;
+    rwt::k_boundaries_mlp<<<ctas, rwt::kBpThreads, 0, s>>>(L->d_sample_sorted, L->d_params,
+                                                          L->group, L->d_bounds);
     RWL_CUDA(cudaGetLastError());
     rwt::k_bounds_monotone<<<1, 1024, 0, s>>>(L->d_bounds);
-  } else
-    rwt::k_boundaries<false><<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->d_params, L->group,
-                                                    L->d_bounds, f);
+  } else if (!features) {
+    rwt::k_boundaries<<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->group, L->d_bounds,
+                                             nullptr);
+  }
   RWL_CUDA(cudaGetLastError());
   return RW_OK;
 }
@@ -673,18 +791,31 @@ int front_half(rw_tree_learned* L, const uint32_t* keys, uint32_t n, bool mlp, b
   return boundaries(L, mlp, features, s);
 }
 
-int counts_and_plan(rw_tree_learned* L, const uint32_t* keys, uint32_t n, cudaStream_t s) {
-  RWL_CUDA(cudaMemsetAsync(L->d_counts, 0, 4 * rwt::kBuckets, s));
+// both split passes into the bucket regions, and the plan; the plan is
+// copied to the host (not waited for)
+int scatter_and_plan(rw_tree_learned* L, const uint32_t* keys, uint32_t n, cudaStream_t s) {
+  const uint32_t cap = rwt::region_cap(n), scap = rwt::super_cap(n);
+  RWL_CUDA(cudaMemsetAsync(L->d_cursor, 0, 4 * rwt::kBuckets, s));
+  RWL_CUDA(cudaMemsetAsync(L->d_super_cursor, 0, 4 * rwt::kSupers, s));
   RWL_CUDA(cudaMemsetAsync(L->d_plan, 0, sizeof(rwt::LearnedPlan), s));
-  const int blocks = std::max(1, std::min<int>(rwt::div_up(n, 512 * 16), L->num_sms * 4));
-  rwt::k_bucket_hist<<<blocks, 512, 0, s>>>(keys, n, L->d_bounds, L->d_counts);
+  const uint32_t tiles1 = rwt::div_up(n, rwt::kSpTile);
+  rwt::k_split<8><<<tiles1, rwt::kSpThreads, rwt::SplitCfg<8>::kSmem, s>>>(
+      keys, n, nullptr, 0, tiles1, 1, L->d_bounds, L->d_super_cursor, L->d_super_region, scap);
   RWL_CUDA(cudaGetLastError());
-  rwt::k_bucket_plan<<<1, 1024, 0, s>>>(L->d_counts, L->d_offsets, L->d_cursor, L->d_plan);
+  const uint32_t tps = rwt::div_up(scap, rwt::kSpTile);
+  rwt::k_split<4><<<rwt::kSupers * tps, rwt::kSpThreads, rwt::SplitCfg<4>::kSmem, s>>>(
+      L->d_super_region, 0, L->d_super_cursor, scap, tps, rwt::kSupers, L->d_bounds, L->d_cursor,
+      L->d_region, cap);
+  RWL_CUDA(cudaGetLastError());
+  rwt::k_bucket_plan<<<1, 1024, 0, s>>>(L->d_cursor, cap, L->d_super_cursor, scap, L->d_offsets,
+                                        L->d_order, L->d_plan);
   RWL_CUDA(cudaGetLastError());
   RWL_CUDA(cudaMemcpyAsync(L->h_plan, L->d_plan, sizeof(rwt::LearnedPlan),
                            cudaMemcpyDeviceToHost, s));
   return RW_OK;
 }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
 
@@ -695,6 +826,8 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
   *out = nullptr;
   auto* L = new rw_tree_learned();
   L->n_max = n_max;
+  L->cap_max = rwt::region_cap(n_max);
+  L->scap_max = rwt::super_cap(n_max);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&L->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -702,10 +835,13 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
     delete L;
     return rc;
   }
-  const size_t words = 2 * size_t(rwt::kSample) + rwt::kBuckets + rwt::kBuckets +
-                       (rwt::kBuckets + 1) + rwt::kBuckets + size_t(n_max) +
-                       rwt::kMlpParams + size_t(rwt::kBounds) * rwt::kMlpIn +
-                       64 /* alignment of the plan */ + 64 /* plan */;
+  auto up = [](size_t words) { return (words + 63) & ~size_t(63); };  // 256-byte pieces
+  const size_t w_sample = up(rwt::kSample), w_b = up(rwt::kBuckets + 1),
+               w_params = up(rwt::kMlpParams), w_feat = up(size_t(rwt::kBounds) * rwt::kMlpIn),
+               w_plan = up(sizeof(rwt::LearnedPlan) / 4),
+               w_region = size_t(rwt::kBuckets) * L->cap_max,
+               w_super = size_t(rwt::kSupers) * L->scap_max;
+  const size_t words = 2 * w_sample + 5 * w_b + w_params + w_feat + w_plan + w_region + w_super;
   cudaError_t e = cudaMalloc(&L->d_mem, 4 * words);
   if (e == cudaSuccess) e = cudaMallocHost(&L->h_plan, sizeof(rwt::LearnedPlan));
   if (e != cudaSuccess) {
@@ -713,27 +849,20 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
     return lfail(e, "rw_tree_learned_create");
   }
   uint32_t* p = static_cast<uint32_t*>(L->d_mem);
-  L->d_sample = p; p += rwt::kSample;
-  L->d_sample_sorted = p; p += rwt::kSample;
-  L->d_bounds = p; p += rwt::kBuckets;
-  L->d_counts = p; p += rwt::kBuckets;
-  L->d_offsets = p; p += rwt::kBuckets + 1;
-  L->d_cursor = p; p += rwt::kBuckets;
-  L->d_params = reinterpret_cast<float*>(p); p += rwt::kMlpParams;
-  L->d_features = reinterpret_cast<float*>(p); p += size_t(rwt::kBounds) * rwt::kMlpIn;
-  p = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(p) + 255) & ~uintptr_t(255));
-  L->d_plan = reinterpret_cast<rwt::LearnedPlan*>(p); p += 64;
-  L->d_tmp = p;
-  if ((reinterpret_cast<uintptr_t>(L->d_tmp) & 15u) != 0) {
-    rw_tree_learned_destroy(L);
-    return RW_ERR_ARG;
-  }
+  L->d_sample = p; p += w_sample;
+  L->d_sample_sorted = p; p += w_sample;
+  L->d_bounds = p; p += w_b;
+  L->d_cursor = p; p += w_b;
+  L->d_offsets = p; p += w_b;
+  L->d_order = p; p += w_b;
+  L->d_super_cursor = p; p += w_b;
+  L->d_params = reinterpret_cast<float*>(p); p += w_params;
+  L->d_features = reinterpret_cast<float*>(p); p += w_feat;
+  L->d_plan = reinterpret_cast<rwt::LearnedPlan*>(p); p += w_plan;
+  L->d_region = p; p += w_region;
+  L->d_super_region = p;
   cudaFuncSetAttribute(rwt::k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        int(rwt::kBsSmem));
-  cudaFuncSetAttribute(rwt::k_bucket_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       int(rwt::kBsSmem));
-  cudaFuncSetAttribute(rwt::k_bucket_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       int(rwt::kScSmem));
   *out = L;
   return RW_OK;
 }
@@ -779,11 +908,12 @@ int rw_tree_learned_features(rw_tree_learned* L, const uint32_t* d_keys, uint32_
 
 int rw_tree_learned_bucket_counts(rw_tree_learned* L, const uint32_t* d_keys, uint32_t n,
                                   int32_t mode, uint32_t* h_counts, rw_stream_t stream) {
-  if (!L || !d_keys || !h_counts || n < rwt::kSample || n > L->n_max) return RW_ERR_ARG;
+  if (!L || !d_keys || !h_counts || n < rwt::kSample || n > L->n_max || !aligned16(d_keys))
+    return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = front_half(L, d_keys, n, mode == RW_LEARNED_MLP, false, s)) return rc;
-  if (int rc = counts_and_plan(L, d_keys, n, s)) return rc;
-  RWL_CUDA(cudaMemcpyAsync(h_counts, L->d_counts, 4 * rwt::kBuckets, cudaMemcpyDeviceToHost, s));
+  if (int rc = scatter_and_plan(L, d_keys, n, s)) return rc;
+  RWL_CUDA(cudaMemcpyAsync(h_counts, L->d_cursor, 4 * rwt::kBuckets, cudaMemcpyDeviceToHost, s));
   RWL_CUDA(cudaStreamSynchronize(s));
   return RW_OK;
 }
@@ -791,7 +921,7 @@ int rw_tree_learned_bucket_counts(rw_tree_learned* L, const uint32_t* d_keys, ui
 int rw_tree_learned_sort(rw_tree_learned* L, const uint32_t* d_keys, uint32_t* d_sorted,
                          uint32_t n, int32_t mode, rw_tree_im_storage* fallback_im,
                          rw_stream_t stream, rw_tree_learned_stats* stats) {
-  if (!L || !d_keys || !d_sorted || n > L->n_max || n < 1 ||
+  if (!L || !d_keys || !d_sorted || n > L->n_max || n < 1 || !aligned16(d_keys) ||
       (mode != RW_LEARNED_MLP && mode != RW_LEARNED_SAMPLE_QUANTILES))
     return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -799,7 +929,7 @@ int rw_tree_learned_sort(rw_tree_learned* L, const uint32_t* d_keys, uint32_t* d
   bool fallback = n < rwt::kSample;
   if (!fallback) {
     if (int rc = front_half(L, d_keys, n, mode == RW_LEARNED_MLP, false, s)) return rc;
-    if (int rc = counts_and_plan(L, d_keys, n, s)) return rc;
+    if (int rc = scatter_and_plan(L, d_keys, n, s)) return rc;
     RWL_CUDA(cudaStreamSynchronize(s));  // the plan decides the path
     fallback = L->h_plan->fallback != 0;
     if (stats) {
@@ -816,18 +946,9 @@ int rw_tree_learned_sort(rw_tree_learned* L, const uint32_t* d_keys, uint32_t* d
     if (stats) stats->fell_back = 1;
     return rw_tree_sort_enqueue(&app, fallback_im, stream);
   }
-  const uint32_t tiles = rwt::div_up(n, rwt::kScTile);
-  rwt::k_bucket_scatter<<<tiles, rwt::kScThreads, rwt::kScSmem, s>>>(d_keys, n, L->d_bounds,
-                                                                     L->d_cursor, L->d_tmp);
+  rwt::k_bucket_sort<<<rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s>>>(
+      L->d_region, rwt::region_cap(n), L->d_cursor, L->d_offsets, L->d_order, d_sorted);
   RWL_CUDA(cudaGetLastError());
-  rwt::k_bucket_sort<<<rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s>>>(L->d_tmp, L->d_offsets,
-                                                                         d_sorted);
-  RWL_CUDA(cudaGetLastError());
-  if (L->h_plan->n_big) {
-    rwt::k_bucket_sort_big<<<rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s>>>(
-        L->d_tmp, d_sorted, L->d_offsets, L->d_counts, d_sorted);
-    RWL_CUDA(cudaGetLastError());
-  }
   return RW_OK;
 }
 

@@ -78,23 +78,43 @@ def test_learned_sort_equals_plain_sort(rw, n):
 
 
 def test_learned_sort_large_bucket_and_fallback(rw):
+    """A bucket above one CTA's capacity takes the chunked path; a bucket above
+    its region (4x the mean bucket size) sends everything to onesweep."""
     torch = _torch()
-    n = 1 << 20
-    L = rw.Learned(4 << 20, params=None)
-    im = rw.ImStorage(4 << 20, 32)
+    n = 1 << 26  # mean bucket 16,384 keys, region 65,536
+    L = rw.Learned(n, params=None)
+    im = rw.ImStorage(n, 32)
     rng = np.random.default_rng(9)
-    # 100K copies of one key: a bucket above one CTA's capacity
     k = rng.integers(0, 1 << 30, n, dtype=np.uint64).astype(np.uint32)
-    k[rng.choice(n, 100_000, replace=False)] = 123456789
+    k[rng.choice(n, 40_000, replace=False)] = 123456789  # one bucket of ~56K keys
     keys = torch.from_numpy(k.view(np.int32)).cuda()
     out, st = L.sort(keys, mode=rw.LEARNED_SAMPLE_QUANTILES, fallback_im=im)
-    assert st["big_buckets"] >= 1 and st["fell_back"] == 0
+    assert st["big_buckets"] >= 1 and st["fell_back"] == 0, st
     assert np.array_equal(out.cpu().numpy().view(np.uint32), np.sort(k))
-    # every key equal: one bucket with everything -> the onesweep sort runs
-    same = torch.full((4 << 20,), 77, dtype=torch.int32, device="cuda")
+    del keys, out
+    # every key equal: one bucket with everything overflows -> onesweep
+    m = 4 << 20
+    same = torch.full((m,), 77, dtype=torch.int32, device="cuda")
     out, st = L.sort(same, mode=rw.LEARNED_SAMPLE_QUANTILES, fallback_im=im)
     assert st["fell_back"] == 1
     assert bool((out == 77).all())
+
+
+def test_bucket_counts_fit_regions(rw):
+    """Trained boundaries on held-out mixtures: counts add up to n and no
+    bucket comes near its region."""
+    from redwood_comp_b200 import learned
+    n = 1 << 24
+    L = rw.Learned(n)
+    cap = 4 * (n // 4096)
+    for seed in (910_001, 910_002):
+        keys = _keys(rw, n, "gauss", seed)
+        for mode in (rw.LEARNED_MLP, rw.LEARNED_SAMPLE_QUANTILES):
+            if mode == rw.LEARNED_MLP and L.params is None:
+                continue
+            c = L.bucket_counts(keys, mode)
+            assert int(c.sum()) == n
+            assert int(c.max()) < cap // 1.2, (seed, mode, int(c.max()))
 
 
 @pytest.mark.parametrize("group", [1, 2, 16])
