@@ -314,6 +314,84 @@ def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
     return info
 
 
+LEARNED_SEED = 950_001  # held out: the boundary MLP trains on seeds 500,000-500,159
+
+
+def measure_learned(rw, a, n=67_108_864, reps=10):
+    """Learned-CDF form: the full pipeline with the learned sort in stage 2
+    against the plain pipeline, 67,108,864 points of a Gaussian mixture with
+    8-64 components (32-bit keys), every output compared on the device."""
+    import torch
+    from redwood_comp_b200 import learned as lmod
+    pts = lmod.mixture_cloud(rw, n, LEARNED_SEED)
+    k_comp = 8 + (LEARNED_SEED * 2654435761 % 57)
+    app_p = rw.AppData(n, 32, points=pts)
+    app_l = rw.AppData(n, 32, points=pts)
+    del pts
+    im_p = rw.ImStorage(n, 32)
+    im_l = rw.ImStorage(n, 32)
+    L = rw.Learned(n)
+    if L.params is None:
+        return {"unavailable": "no trained boundary MLP table"}
+    s = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(k):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    plain_ms = timed(lambda: rw.pipeline_enqueue(app_p, im_p), reps)
+    rw.pipeline_finish(app_p, im_p)
+    out = {}
+    for mode, name in ((rw.LEARNED_MLP, "mlp"), (rw.LEARNED_SAMPLE_QUANTILES, "sample_quantiles")):
+        im_l.set_learned(L, mode)
+        ms = timed(lambda: rw.pipeline_enqueue(app_l, im_l), reps)
+        rw.pipeline_finish(app_l, im_l)
+        same = app_l.get_n_unique() == app_p.get_n_unique() and \
+            app_l.get_n_octree_nodes() == app_p.get_n_octree_nodes()
+        mism = []
+        for f in ("u_morton_keys_alt", "brt_prefix_n", "brt_has_leaf_left", "brt_has_leaf_right",
+                  "brt_left_child", "brt_parents", "u_edge_count", "u_edge_offset",
+                  "oct_children", "oct_corner", "oct_cell_size", "oct_child_node_mask",
+                  "oct_child_leaf_mask"):
+            x, y = getattr(app_l, f), getattr(app_p, f)
+            if f.startswith("oct_"):
+                x, y = x[:app_p.get_n_octree_nodes()], y[:app_p.get_n_octree_nodes()]
+            elif not f.startswith("u_morton"):
+                x, y = x[:app_p.get_n_unique()], y[:app_p.get_n_unique()]
+            if not torch.equal(x, y):
+                mism.append(f)
+        out[name] = {"value": n / (ms / 1e3), "ms_per_step": ms,
+                     "speedup_vs_plain": plain_ms / ms, "stats": im_l.learned_stats(),
+                     "mismatched_outputs_vs_plain": mism if same else ["counts"] + mism}
+    im_l.set_learned(None)
+    # the sort alone, same keys
+    keys = app_p.u_morton_keys.clone()
+    sorted_out = torch.empty_like(keys)
+    sort_ms = {"onesweep": timed(lambda: rw.sort_keys(keys, sorted_out, im_p), reps)}
+    for mode, name in ((rw.LEARNED_MLP, "learned_mlp"),
+                       (rw.LEARNED_SAMPLE_QUANTILES, "learned_sample_quantiles")):
+        sort_ms[name] = timed(lambda: L.sort(keys, out=sorted_out, mode=mode, fallback_im=im_p),
+                              reps)
+    info = {
+        "workload": f"learned-CDF: {n:,} points, Gaussian mixture with {k_comp} components "
+                    f"(sigma 4-40, seed {LEARNED_SEED}, not a training seed), 32-bit keys",
+        "plain_value": n / (plain_ms / 1e3), "plain_ms_per_step": plain_ms,
+        "learned": out, "sort_only_ms": {k: round(v, 4) for k, v in sort_ms.items()},
+        "boundary_mlp": {"group": L.group, "params": int(L.params.size)},
+        "unit": "points/s",
+    }
+    L.close()
+    return info
+
+
 def cpu_baseline(rw, pts, a):
     from oracle import RefTree, ref_available
     if a.key_bits != 32 or not ref_available():
@@ -476,6 +554,8 @@ def main():
         del app, im
         torch.cuda.empty_cache()
         forms = {"batched": measure_batch(rw, a)}
+        torch.cuda.empty_cache()
+        forms["learned"] = measure_learned(rw, a)
 
     if world > 1:
         dist.destroy_process_group()

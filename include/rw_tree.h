@@ -341,6 +341,19 @@ int rw_tree_learned_features(rw_tree_learned* learned, const uint32_t* d_keys, u
 int rw_tree_learned_bucket_counts(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t n,
                                   int32_t mode, uint32_t* counts, rw_stream_t stream);
 
+/* Stage 2 of this scratch's pipeline (rw_tree_run_stage2 and
+ * rw_tree_pipeline_enqueue) sorts with `learned` in `mode` instead of the
+ * onesweep sort; NULL restores onesweep.  32-bit keys only; `learned` must
+ * serve n_input keys and outlive its use here.  The pipeline then waits once
+ * for the learned sort's bucket plan inside rw_tree_pipeline_enqueue, and
+ * rw_tree_pipeline_profile reports "morton,learned_sort,..." (7 entries).
+ * The output is bit-identical either way. */
+int rw_tree_im_storage_set_learned(rw_tree_im_storage* im, rw_tree_learned* learned,
+                                   int32_t mode);
+/* The learned sort's statistics of the last run on this scratch. */
+int rw_tree_im_storage_learned_stats(const rw_tree_im_storage* im,
+                                     rw_tree_learned_stats* out);
+
 /* Training kernels of the boundary MLP (device arrays).  x: [rows][16],
  * t: [rows]; mean squared error over `batch` examples (rows of this call may
  * be a part of the batch).  grad and loss_sum are accumulated into. */

@@ -104,7 +104,8 @@ EXPORTS = (
     "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
     "rw_tree_sort_profile",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
-    "rw_tree_learned_set_group",
+    "rw_tree_learned_set_group", "rw_tree_im_storage_set_learned",
+    "rw_tree_im_storage_learned_stats",
     "rw_tree_learned_sort", "rw_tree_learned_features", "rw_tree_learned_bucket_counts",
     "rw_tree_mlp_param_count", "rw_tree_mlp_grad", "rw_tree_mlp_adam", "rw_tree_mlp_forward",
 )
@@ -191,6 +192,20 @@ class ImStorage:
     def set_sort_variant(self, idx: int) -> None:
         _check(lib().rw_tree_im_storage_set_sort_variant(self._h, idx), "set_sort_variant")
         self.sort_variant = idx
+
+    def set_learned(self, learned, mode: int = 0) -> None:
+        """Stage 2 sorts with the learned-CDF sort `learned` (a Learned, or
+        None for the onesweep sort); 32-bit keys only."""
+        _check(lib().rw_tree_im_storage_set_learned(
+            self._h, learned._h if learned is not None else None, ctypes.c_int32(mode)),
+            "set_learned")
+        self.learned = learned
+
+    def learned_stats(self) -> dict:
+        st = _LearnedStatsC()
+        _check(lib().rw_tree_im_storage_learned_stats(self._h, ctypes.byref(st)), "learned_stats")
+        return {"max_bucket": st.max_bucket, "big_buckets": st.big_buckets,
+                "fell_back": st.fell_back}
 
     def clear(self, stream=None) -> None:
         _check(lib().rw_tree_im_storage_clear(self._h, _stream_handle(stream)), "clearSmem")

@@ -294,6 +294,13 @@ int rw_tree_run_stage2(rw_tree_app_data* app, rw_tree_im_storage* im,
   const auto b = bufs_of(*app, im);
   const auto sc = scratch_of(im);
   const auto pl = plan_of(*app, im);
+  if (im->learned) {
+    if (int rc = rw_tree_learned_sort(im->learned, static_cast<const uint32_t*>(b.keys),
+                                      static_cast<uint32_t*>(b.alt), app->n_input,
+                                      im->learned_mode, im, stream, &im->learned_stats))
+      return rc;
+    return sync_status(im, s);
+  }
   RW_CUDA(rwt::launch_keys(b, sc, pl, false, true, s));
   RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s));
   return sync_status(im, s);
@@ -433,10 +440,23 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
   const auto sc = scratch_of(im);
   const auto pl = plan_of(*app, im);
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_keys(b, sc, pl, true, true, s));
-  RW_CUDA(mark());
-  RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s, ev ? ev + k : nullptr));
-  if (ev) k += 1 + im->passes;
+  if (im->learned) {
+    // stage 1 without the digit histograms, then the learned-CDF sort (which
+    // waits for its bucket plan once, and falls back to onesweep on `im`)
+    RW_CUDA(rwt::launch_keys(b, sc, pl, true, false, s));
+    RW_CUDA(mark());
+    if (int rc = rw_tree_learned_sort(im->learned, static_cast<const uint32_t*>(b.keys),
+                                      static_cast<uint32_t*>(b.alt), app->n_input,
+                                      im->learned_mode, im, reinterpret_cast<rw_stream_t>(s),
+                                      &im->learned_stats))
+      return rc;
+    RW_CUDA(mark());
+  } else {
+    RW_CUDA(rwt::launch_keys(b, sc, pl, true, true, s));
+    RW_CUDA(mark());
+    RW_CUDA(rwt::launch_sort_passes(b, sc, pl, s, ev ? ev + k : nullptr));
+    if (ev) k += 1 + im->passes;
+  }
   RW_CUDA(rwt::launch_unique(b, sc, pl, s));
   RW_CUDA(mark());
   RW_CUDA(rwt::launch_radix_tree(b, sc, pl, true, s));
@@ -460,10 +480,31 @@ int rw_tree_pipeline_enqueue(rw_tree_app_data* app, rw_tree_im_storage* im,
 
 const char* rw_tree_pipeline_kernel_names(const rw_tree_im_storage* im) {
   static thread_local std::string names;
-  names = "morton_histogram,sort_init";
-  for (int p = 0; p < (im ? im->passes : 0); ++p) names += ",sort_pass" + std::to_string(p);
+  if (im && im->learned) {
+    names = "morton,learned_sort";
+  } else {
+    names = "morton_histogram,sort_init";
+    for (int p = 0; p < (im ? im->passes : 0); ++p) names += ",sort_pass" + std::to_string(p);
+  }
   names += ",unique,radix_tree_edges,edge_scan,octree_rows,octree_links";
   return names.c_str();
+}
+
+int rw_tree_im_storage_set_learned(rw_tree_im_storage* im, rw_tree_learned* learned,
+                                   int32_t mode) {
+  if (!im || (mode != RW_LEARNED_MLP && mode != RW_LEARNED_SAMPLE_QUANTILES) ||
+      (learned && im->key_bits != 32))
+    return RW_ERR_ARG;
+  im->learned = learned;
+  im->learned_mode = mode;
+  im->learned_stats = rw_tree_learned_stats{};
+  return RW_OK;
+}
+
+int rw_tree_im_storage_learned_stats(const rw_tree_im_storage* im, rw_tree_learned_stats* out) {
+  if (!im || !out) return RW_ERR_ARG;
+  *out = im->learned_stats;
+  return RW_OK;
 }
 
 int rw_tree_pipeline_profile(rw_tree_app_data* app, rw_tree_im_storage* im,
@@ -471,7 +512,7 @@ int rw_tree_pipeline_profile(rw_tree_app_data* app, rw_tree_im_storage* im,
                              int32_t max_kernels, int32_t* n_kernels) {
   if (!app || !im || !kernel_ms || reps < 1) return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int n_k = 7 + im->passes;
+  const int n_k = 7 + (im->learned ? 0 : im->passes);
   if (max_kernels < n_k) return RW_ERR_ARG;
   cudaEvent_t ev[64];
   for (int i = 0; i <= n_k; ++i) RW_CUDA(cudaEventCreate(&ev[i]));

@@ -39,6 +39,11 @@ struct rw_tree_im_storage {
   size_t sort_zero_off = 0, sort_zero_bytes = 0;  // ghist + sort_desc
 
   rwt::DevStatus* h_status = nullptr;  // pinned mirror
+
+  // optional learned-CDF sort for stage 2 (32-bit keys); not owned
+  rw_tree_learned* learned = nullptr;
+  int32_t learned_mode = 0;
+  rw_tree_learned_stats learned_stats{};
 };
 
 namespace rwt {

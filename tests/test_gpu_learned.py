@@ -153,3 +153,25 @@ def test_features_match_numpy_restatement(rw, group):
     np.testing.assert_allclose(f[rows], np.concatenate([coarse, fine], 1), rtol=4e-7, atol=1e-7)
     others = np.setdiff1d(np.arange(4095), rows)
     assert np.all(f[others] == 0)
+
+
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_pipeline_with_learned_sort_matches_oracle(rw, oracle, fused, mode):
+    """Stage 2 by the learned sort (set on the pipeline's scratch): all seven
+    stages stay bit-exact against the oracle, fused and stage by stage."""
+    from redwood_comp_b200 import learned
+    from test_gpu_parity import run_gpu, assert_same
+    n = 1_000_003
+    pts = learned.mixture_cloud(rw, n, 20_017)
+    L = rw.Learned(n)
+    if L.params is None:
+        L.set_params(learned.init_params(1))
+    im = rw.ImStorage(n, 32)
+    im.set_learned(L, mode)
+    got = run_gpu(rw, pts, fused=fused, im=im)
+    assert im.learned_stats()["fell_back"] == 0
+    assert_same(got, oracle.run(pts, key_bits=32), f"learned mode {mode} fused {fused}")
+    # back to onesweep on the same scratch
+    im.set_learned(None)
+    assert_same(run_gpu(rw, pts, fused=fused, im=im), oracle.run(pts, key_bits=32), "onesweep")
