@@ -2,8 +2,9 @@
 // scan, octree.
 //
 // Stage 3 replaces k_FindDups + host std::partial_sum + k_MoveDups
-// (apps/tree/cuda/03_unique.cu, cu_dispatcher.cu:597-627) with one kernel:
-// ballot head flags, a block scan and a warp-cooperative decoupled look-back.
+// (apps/tree/cuda/03_unique.cu, cu_dispatcher.cu:597-627) with two launches:
+// per-tile ballot head counts scanned by the last block to finish, then a
+// compaction of every tile at its scanned offset.
 //
 // Stage 4 is process_radix_tree_i of apps/tree/host/func_brt.hpp:45-138,
 // one thread per node.  The parent writes are made deterministic (see
@@ -38,76 +39,132 @@ namespace rwt {
 // stage 3: unique
 // ---------------------------------------------------------------------------
 
+// Stage 3 in two launches without a serial chain between tiles: (1) every
+// tile counts its heads (a key is a head when it differs from its left
+// neighbour in the segment, or starts the segment) into E[tile]; the block
+// that finishes last turns E into its exclusive scan (E[tiles] = total) and
+// writes each segment's n_unique; (2) every tile compacts its heads to
+// segment begin + E[tile] - E[first tile of the segment].  Same result as
+// cu_dispatcher.cu:597-627 (a std::unique over the sorted keys).
+template <typename K>
+__device__ __forceinline__ uint32_t tile_heads(const K* __restrict__ sorted, uint32_t sb,
+                                               uint32_t n, uint32_t wbase,
+                                               K (&keys)[kUniqueKpt],
+                                               uint32_t (&heads)[kUniqueKpt]) {
+  const uint32_t lane = lane_id();
+  K carry = K(0);
+  uint32_t count = 0;
+#pragma unroll
+  for (int i = 0; i < kUniqueKpt; ++i) {
+    const uint32_t idx = wbase + 32u * i + lane;
+    const K k = idx < n ? sorted[idx] : K(0);
+    K left = __shfl_up_sync(0xffffffffu, k, 1);
+    if (lane == 0) {
+      if (i == 0)
+        left = (wbase > sb && wbase - 1 < n) ? sorted[wbase - 1] : K(~k);
+      else
+        left = carry;
+    }
+    carry = __shfl_sync(0xffffffffu, k, 31);
+    const bool head = idx < n && (idx == sb || k != left);
+    heads[i] = __ballot_sync(0xffffffffu, head);
+    keys[i] = k;
+    count += __popc(heads[i]);
+  }
+  return count;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
-    k_unique(const K* __restrict__ sorted, K* __restrict__ out, SegTable seg, TileMap map,
-             uint32_t* __restrict__ n_unique, uint32_t* __restrict__ desc,
-             uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
-  constexpr int KPT = kUniqueKpt, NW = kUniqueThreads / 32;
+    k_unique_count(const K* __restrict__ sorted, SegTable seg, TileMap map,
+                   uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E,
+                   uint32_t* __restrict__ done) {
+  constexpr int NW = kUniqueThreads / 32;
   __shared__ uint32_t s_warp[NW + 1];
-  __shared__ uint32_t s_tile, s_excl;
-  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  while (true) {
-    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= map.n_tiles) break;
-    uint32_t first;
-    const uint32_t c = tile_segment(seg, map, tile, &first);
-    const uint32_t sb = seg_begin(seg, c);
-    const uint32_t n = sb + seg_size(seg, c);  // end of the segment
-    const uint32_t last = map.toff ? map.toff[c + 1] - 1 : map.n_tiles - 1;
-    const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * KPT;
-    K keys[KPT];
-    uint32_t heads[KPT];
-    K carry = K(0);
-    uint32_t count = 0;
+  __shared__ bool s_last;
+  const uint32_t tile = blockIdx.x, lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, tile, &first);
+  const uint32_t sb = seg_begin(seg, c);
+  const uint32_t n = sb + seg_size(seg, c);
+  const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * kUniqueKpt;
+  K keys[kUniqueKpt];
+  uint32_t heads[kUniqueKpt];
+  const uint32_t count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  if (lane == 0) s_warp[warp] = count;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < NW; ++w) t += s_warp[w];
+    E[tile] = t;
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  // the last block: exclusive scan of E[0, tiles) in place, in chunks of
+  // kUniqueThreads * 8 (every other block's count is visible: each fenced
+  // its write before its increment of `done`)
+  __threadfence();
+  constexpr int R = 8;
+  const uint32_t tiles = gridDim.x;
+  uint32_t carry = 0;
+  for (uint32_t c0 = 0; c0 < tiles; c0 += kUniqueThreads * R) {
+    const uint32_t f = c0 + threadIdx.x * R;
+    uint32_t v[R], local = 0;
 #pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const uint32_t idx = wbase + 32u * i + lane;
-      const K k = idx < n ? sorted[idx] : K(0);
-      K left = __shfl_up_sync(0xffffffffu, k, 1);
-      if (lane == 0) {
-        if (i == 0)
-          left = (wbase > sb && wbase - 1 < n) ? sorted[wbase - 1] : K(~k);
-        else
-          left = carry;
-      }
-      carry = __shfl_sync(0xffffffffu, k, 31);
-      const bool head = idx < n && (idx == sb || k != left);
-      heads[i] = __ballot_sync(0xffffffffu, head);
-      keys[i] = k;
-      count += __popc(heads[i]);
+    for (int r = 0; r < R; ++r) {
+      v[r] = f + r < tiles ? __ldcg(E + f + r) : 0u;
+      local += v[r];
     }
-    if (lane == 0) s_warp[warp] = count;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t cw = lane < NW ? s_warp[lane] : 0u;
-      const uint32_t inc = warp_inclusive_scan(cw);
-      if (lane < NW) s_warp[lane] = inc - cw;
-      const uint32_t total = __shfl_sync(0xffffffffu, inc, NW - 1);
-      uint32_t excl = 0;
-      if (tile == first) {
-        if (lane == 0) st_relaxed(desc + tile, kFlagInc | (total << 2));
-      } else {
-        if (lane == 0) st_relaxed(desc + tile, kFlagAgg | (total << 2));
-        excl = warp_lookback(desc, tile, st, kSiteUnique, first);
-        if (lane == 0) st_relaxed(desc + tile, kFlagInc | ((excl + total) << 2));
-      }
-      if (lane == 0) {
-        s_excl = excl;
-        if (tile == last) n_unique[c] = excl + total;
-      }
-    }
-    __syncthreads();
-    uint32_t pos = sb + s_excl + s_warp[warp];
+    uint32_t total;
+    uint32_t run = carry + block_exclusive_scan<kUniqueThreads>(local, s_warp, &total);
 #pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const uint32_t dst = pos + __popc(heads[i] & lanemask_lt());
-      if (((heads[i] >> lane) & 1u) && dst < n) out[dst] = keys[i];
-      pos += __popc(heads[i]);
+    for (int r = 0; r < R; ++r) {
+      if (f + r < tiles) E[f + r] = run;
+      run += v[r];
     }
-    __syncthreads();
+    carry += total;
+  }
+  if (threadIdx.x == 0) E[tiles] = carry;
+  __syncthreads();
+  __threadfence_block();
+  for (uint32_t sg = threadIdx.x; sg < seg.count; sg += kUniqueThreads) {
+    const uint32_t t0 = map.toff ? map.toff[sg] : 0u;
+    const uint32_t t1 = map.toff ? map.toff[sg + 1] : tiles;
+    n_unique[sg] = (t1 < tiles ? E[t1] : carry) - (t0 < tiles ? E[t0] : carry);
+  }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kUniqueThreads)
+    k_unique_write(const K* __restrict__ sorted, K* __restrict__ out, SegTable seg, TileMap map,
+                   const uint32_t* __restrict__ E) {
+  constexpr int NW = kUniqueThreads / 32;
+  __shared__ uint32_t s_warp[NW];
+  const uint32_t tile = blockIdx.x, lane = lane_id(), warp = threadIdx.x >> 5;
+  uint32_t first;
+  const uint32_t c = tile_segment(seg, map, tile, &first);
+  const uint32_t sb = seg_begin(seg, c);
+  const uint32_t n = sb + seg_size(seg, c);
+  const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * kUniqueKpt;
+  K keys[kUniqueKpt];
+  uint32_t heads[kUniqueKpt];
+  const uint32_t count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  if (lane == 0) s_warp[warp] = count;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t cw = lane < NW ? s_warp[lane] : 0u;
+    const uint32_t inc = warp_inclusive_scan(cw);
+    if (lane < NW) s_warp[lane] = inc - cw;
+  }
+  __syncthreads();
+  uint32_t pos = sb + (E[tile] - E[first]) + s_warp[warp];
+#pragma unroll
+  for (int i = 0; i < kUniqueKpt; ++i) {
+    const uint32_t dst = pos + __popc(heads[i] & lanemask_lt());
+    if (((heads[i] >> lane) & 1u) && dst < n) out[dst] = keys[i];
+    pos += __popc(heads[i]);
   }
 }
 
@@ -575,10 +632,11 @@ template <typename K>
 cudaError_t unique_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
   const uint32_t tiles = pl.unique_map.n_tiles;
   if (!tiles) return cudaSuccess;
-  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(sc, 8)));
-  k_unique<K><<<blocks, kUniqueThreads, 0, s>>>(
-      static_cast<const K*>(b.alt), static_cast<K*>(b.keys), pl.seg, pl.unique_map,
-      pl.n_unique, sc.unique_desc, sc.tile_ctr + kCtrUnique, sc.status);
+  const K* sorted = static_cast<const K*>(b.alt);
+  k_unique_count<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, pl.seg, pl.unique_map, pl.n_unique,
+                                                     sc.unique_desc, sc.tile_ctr + kCtrUnique);
+  k_unique_write<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, static_cast<K*>(b.keys), pl.seg,
+                                                     pl.unique_map, sc.unique_desc);
   return cudaGetLastError();
 }
 

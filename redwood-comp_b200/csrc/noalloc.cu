@@ -28,7 +28,7 @@ constexpr uint32_t kMaxTiles = (kMaxKeys + rwt::kUniqueTile - 1) / rwt::kUniqueT
 // [0, 256): DevStatus, then the tile ticket at 256; look-back words from 512.
 constexpr size_t kTicketOffset = 256;
 constexpr size_t kDescOffset = 512;
-constexpr size_t kScratchBytes = kDescOffset + size_t(kMaxTiles) * 4;
+constexpr size_t kScratchBytes = kDescOffset + (size_t(kMaxTiles) + 1) * 4;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -78,7 +78,7 @@ extern "C" int rw_tree_unique_noalloc(const void* sorted_keys, void* unique_keys
   const uint32_t tiles = (n + rwt::kUniqueTile - 1) / rwt::kUniqueTile;
   // the array keeps the previous call's words: the ticket, the status and the
   // look-back words of this call's tiles must start at zero
-  if (cudaMemsetAsync(base, 0, kDescOffset + size_t(tiles) * 4, s) != cudaSuccess)
+  if (cudaMemsetAsync(base, 0, kDescOffset + (size_t(tiles) + 1) * 4, s) != cudaSuccess)
     return RW_ERR_CUDA;
   if (rwt::launch_unique_raw(sorted_keys, unique_keys, n, key_bits, desc, ticket, status,
                              num_sms, s) != cudaSuccess)
