@@ -47,6 +47,8 @@ struct rw_tree_batch {
   uint32_t* d_class_toff = nullptr;                  // [kMaxSortClasses][n_clouds + 1]
 
   void* d_tmp_keys = nullptr;
+  uint32_t* d_tree_far = nullptr;  // radix-tree far-search list
+  uint32_t tree_far_cap = 0;
   void* d_zero = nullptr;
   size_t zero_bytes = 0;
   uint32_t *d_ghist = nullptr, *d_sort_desc = nullptr, *d_unique_desc = nullptr,
@@ -154,6 +156,8 @@ rwt::Scratch scratch_of(const rw_tree_batch* b) {
   sc.scan_desc = b->d_scan_desc;
   sc.tile_ctr = b->d_tile_ctr;
   sc.status = b->d_status;
+  sc.tree_far = b->d_tree_far;
+  sc.tree_far_cap = b->tree_far_cap;
   return sc;
 }
 
@@ -276,6 +280,8 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   const size_t ks = key_bits == 32 ? 4 : 8;
   cudaError_t e = cudaMalloc(&b->d_tables, (8 + rwt::kMaxSortClasses) * tab * 4);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tmp_keys, ks * total);
+  b->tree_far_cap = b->tree_tiles * rwt::kTreeFarPerTile;
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_tree_far, size_t(b->tree_far_cap) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_zero, b->zero_bytes);
   if (e == cudaSuccess) e = cudaMallocHost(&b->h_results, (3 * size_t(n_clouds) + 4) * 4);
   if (e != cudaSuccess) {
@@ -325,6 +331,7 @@ int rw_tree_batch_destroy(rw_tree_batch* b) {
   release_stream(b);
   if (b->d_tables) cudaFree(b->d_tables);
   if (b->d_tmp_keys) cudaFree(b->d_tmp_keys);
+  if (b->d_tree_far) cudaFree(b->d_tree_far);
   if (b->d_zero) cudaFree(b->d_zero);
   if (b->h_results) cudaFreeHost(b->h_results);
   delete b;

@@ -104,6 +104,8 @@ rwt::Scratch scratch_of(const rw_tree_im_storage* im) {
   sc.scan_desc = im->d_scan_desc;
   sc.tile_ctr = im->d_tile_ctr;
   sc.status = im->d_status;
+  sc.tree_far = im->d_tree_far;
+  sc.tree_far_cap = im->tree_far_cap;
   return sc;
 }
 
@@ -216,6 +218,8 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
 
   cudaError_t e = cudaMalloc(&im->d_zero, im->zero_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&im->d_tmp_keys, key_size(key_bits) * n_input);
+  im->tree_far_cap = rwt::div_up(n_input, rwt::kTreeTile) * rwt::kTreeFarPerTile;
+  if (e == cudaSuccess) e = cudaMalloc(&im->d_tree_far, size_t(im->tree_far_cap) * 8);
   if (e == cudaSuccess) e = cudaMallocHost(&im->h_status, sizeof(rwt::DevStatus));
   if (e != cudaSuccess) {
     rw_tree_im_storage_destroy(im);
@@ -264,6 +268,7 @@ int rw_tree_im_storage_destroy(rw_tree_im_storage* im) {
   if (!im) return RW_OK;
   if (im->d_zero) cudaFree(im->d_zero);
   if (im->d_tmp_keys) cudaFree(im->d_tmp_keys);
+  if (im->d_tree_far) cudaFree(im->d_tree_far);
   if (im->h_status) cudaFreeHost(im->h_status);
   delete im;
   return RW_OK;

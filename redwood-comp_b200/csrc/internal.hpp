@@ -26,6 +26,8 @@ struct rw_tree_im_storage {
   uint32_t sort_tiles = 0;  // tiles per pass at n_cap
 
   void* d_tmp_keys = nullptr;  // [n_cap] ping-pong buffer of the sort
+  uint32_t* d_tree_far = nullptr;  // radix-tree gaps left to the far search
+  uint32_t tree_far_cap = 0;       // entries (two words each)
 
   // zero region
   void* d_zero = nullptr;
@@ -57,8 +59,8 @@ constexpr uint32_t kUniqueThreads = 256, kUniqueKpt = 16;
 constexpr uint32_t kUniqueTile = kUniqueThreads * kUniqueKpt;
 constexpr uint32_t kScanThreads = 256, kScanKpt = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanKpt;
-constexpr int kTreeThreads = 256, kTreeNpt = 4, kTreeHalo = 256;
-constexpr uint32_t kTreeTile = kTreeThreads * kTreeNpt;
+constexpr int kTreeThreads = 256;
+constexpr uint32_t kTreeTile = 2048;  // radix-tree nodes (key gaps) per tile
 constexpr int kOctThreads = 256, kOctNpt = 4;
 constexpr uint32_t kOctTile = kOctThreads * kOctNpt;
 
@@ -111,7 +113,14 @@ struct Scratch {
   uint32_t* scan_desc = nullptr;
   uint32_t* tile_ctr = nullptr;
   DevStatus* status = nullptr;
+  uint32_t* tree_far = nullptr;  // [tree_far_cap][2]: segment-global gap, segment
+  uint32_t tree_far_cap = 0;
 };
+
+// Entries of the radix tree's far-search list per tile: the gaps of a tile
+// with no smaller gap inside its window have strictly decreasing (left side)
+// or increasing (right side) prefix lengths, so there are at most 64 per side.
+constexpr uint32_t kTreeFarPerTile = 128;
 
 // Segments and the tile map of every kernel, plus per-segment results.
 struct Plan {

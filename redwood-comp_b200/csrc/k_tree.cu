@@ -181,20 +181,6 @@ struct BrtNode {
   int d, j, gamma, dnode;
 };
 
-// Key reads of the radix-tree search go through a shared-memory window of the
-// tile's keys plus a halo on either side; probes outside it read global memory.
-template <typename K>
-struct KeyWindow {
-  const K* __restrict__ codes;
-  const K* win;  // shared memory
-  int lo;        // global index of win[0]
-  int len;
-  __device__ __forceinline__ K operator()(int j) const {
-    const int r = j - lo;
-    return uint32_t(r) < uint32_t(len) ? win[r] : codes[j];
-  }
-};
-
 // delta(a, b) > d, for codes whose top bit is clear (the reference asserts it,
 // func_brt.hpp:30-31): clz(a ^ b) - 1 > d  <=>  a ^ b < 2^(W - 2 - d).  `lim`
 // is that bound (0 when d >= W - 1: never true).
@@ -291,21 +277,153 @@ __device__ __forceinline__ void seg_error(int32_t* seg_err, uint32_t c, int32_t 
   atomicCAS(reinterpret_cast<int*>(seg_err + c), 0, code);
 }
 
-// One CTA per tile of kTreeTile nodes (the tile map is sized by points, an
-// upper bound of the nodes); node base + q*kTreeThreads + tid for q <
-// kTreeNpt (striped, so every store instruction of a warp is contiguous).
-// With EDGES the kernel also writes edge_count (stages 4 and 5 in one pass);
-// tiles are independent, so no CTA ever waits for another.
+// Key reads of node 0's searches: global memory only.
+template <typename K>
+struct GlobalKeys {
+  const K* __restrict__ codes;
+  __device__ __forceinline__ K operator()(int j) const { return codes[j]; }
+};
+
+// ---- stages 4 (+5) from nearest smaller values ----------------------------
+//
+// With D[k] = delta(key k, key k+1) for the n gaps k in [0, n), the binary
+// radix tree of the keys is the Cartesian tree of D: the node that splits at
+// gap g covers keys [L+1, R], where L < g and R > g are the nearest gaps with
+// D strictly smaller than D[g] (-1 and n when there are none); its prefix
+// length is D[g]; its parent splits at whichever of L, R has the larger D; and
+// its Karras index (the one process_radix_tree_i gives it, func_brt.hpp:45-138)
+// is R when it is its parent's left child and L+1 when it is the right child.
+// Every node's outputs follow without a search: left_child = g, leaf flags
+// g == L+1 and g+1 == R, the internal children's parent links, and the edge
+// count from the parent's prefix max(D[L], D[R]).  The root (L = -1, R = n)
+// is node 0, which keeps the reference's own computation over [0, n-1]
+// (brt_node / write_node above).
+//
+// L and R per gap: in chunks of 32 gaps (one per lane) a bit-serial warp
+// comparison of E = D + 1 (0 marks the walls at -1 and n) gives every lane
+// the lanes with a smaller value, hence the nearest smaller in the chunk, and
+// every value v the last / first position in the chunk below v.  Across the
+// tile and a halo of kAnsvHalo chunks on either side, a prefix maximum and a
+// suffix minimum of those summaries answer the rest; a gap whose nearest
+// smaller lies beyond the halo (a node near the top of the tree) searches the
+// keys in global memory.
+constexpr int kAnsvHalo = 8;                                        // chunks per side
+constexpr int kAnsvChunks = int(kTreeTile) / 32 + 2 * kAnsvHalo;   // chunks per window
+constexpr int kAnsvWin = kAnsvChunks * 32;                           // gaps per window
+constexpr int kAnsvRow = kAnsvChunks + 1;  // padded: lane v and chunk c in different banks
+constexpr int kAnsvNone = -0x7fffffff;     // "no smaller gap found to the left"
+constexpr int kAnsvNoneR = 0x7fffffff;     // "none to the right"
+
+template <typename K>
+struct AnsvCfg {
+  static constexpr int NV = sizeof(K) == 4 ? 32 : 64;  // values of E
+  static constexpr int VB = sizeof(K) == 4 ? 5 : 6;    // bits of E
+  static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
+  static constexpr size_t kSmem = kKeyBytes + 2 * size_t(NV) * kAnsvRow * 4 +
+                                  2 * size_t(kTreeTile) * 4 + size_t(kAnsvWin);
+};
+
+// Warp-cooperative searches for the nearest smaller gap of gap g beyond any
+// window: 32 probes per round (doubling distances, then 32-ary refinement), so
+// a search costs about six dependent loads.  pred(a) = delta(key a, key g) > D
+// is true from some a_min up to g; returns a_min (the node's first key).
+template <typename K>
+__device__ int coop_first_key(const K* __restrict__ codes, int g, int D) {
+  const uint32_t lane = lane_id();
+  const K cg = codes[g], lim = delta_limit<K>(D);
+  const int p = lane < 31 ? g - (1 << lane) : -1;
+  const bool f = p >= 0 && (codes[p] ^ cg) < lim;
+  const int js = __ffs(__ballot_sync(0xffffffffu, !f)) - 1;  // a false probe exists
+  int lo = max(js < 31 ? g - (1 << js) : -1, -1);                // pred(lo) false
+  int hi = js == 0 ? g : g - (1 << (js - 1));                    // pred(hi) true
+  while (hi - lo > 1) {
+    const int step = (hi - lo + 31) / 32;
+    const int q = lo + (int(lane) + 1) * step;
+    const bool in = lane < 31 && q < hi;
+    const bool t = in && (codes[q] ^ cg) < lim;
+    const uint32_t mt = __ballot_sync(0xffffffffu, t), mi = __ballot_sync(0xffffffffu, in);
+    if (mt) {
+      const int ft = __ffs(mt) - 1;
+      hi = lo + (ft + 1) * step;
+      lo = ft > 0 ? lo + ft * step : lo;
+    } else {
+      lo = lo + (32 - __clz(mi)) * step;  // the last probe in range is false
+    }
+  }
+  return hi;
+}
+
+// pred(b) = delta(key g+1, key b) > D is true from g+1 up to some b_max <= n;
+// returns b_max (the node's last key).
+template <typename K>
+__device__ int coop_last_key(const K* __restrict__ codes, int n, int g, int D) {
+  const uint32_t lane = lane_id();
+  const K cg = codes[g + 1], lim = delta_limit<K>(D);
+  const long long p = lane < 31 ? (long long)g + 1 + (1ll << lane) : (long long)n + 1;
+  const bool f = p <= n && (codes[int(p)] ^ cg) < lim;
+  const int js = __ffs(__ballot_sync(0xffffffffu, !f)) - 1;
+  int hi = js < 31 ? int(min((long long)g + 1 + (1ll << js), (long long)n + 1)) : n + 1;
+  int lo = js == 0 ? g + 1 : g + 1 + (1 << (js - 1));            // pred(lo) true
+  while (hi - lo > 1) {
+    const int step = (hi - lo + 31) / 32;
+    const int q = lo + (int(lane) + 1) * step;
+    const bool in = lane < 31 && q < hi;
+    const bool t = in && (codes[q] ^ cg) < lim;
+    const uint32_t mf = __ballot_sync(0xffffffffu, in && !t), mi = __ballot_sync(0xffffffffu, in);
+    if (mf) {
+      const int ff = __ffs(mf) - 1;
+      hi = lo + (ff + 1) * step;
+      lo = ff > 0 ? lo + ff * step : lo;
+    } else {
+      lo = lo + (32 - __clz(mi)) * step;  // every probe in range is true
+    }
+  }
+  return lo;
+}
+
+// Writes the node that splits at gap g, given its nearest smaller gaps L, R
+// (see the ANSV comment below); the root (L = -1, R = n) is skipped.
+template <typename K, bool EDGES, typename DAt>
+__device__ __forceinline__ void write_gap_node(int g, int n, int D, int L, int R, const DAt& d_at,
+                                               int root_true_delta, int root_prefix,
+                                               uint8_t* pn, uint8_t* l8, uint8_t* r8,
+                                               int32_t* lcs, int32_t* par, int32_t* ec) {
+  if (L < 0 && R >= n) return;
+  const int dl = L >= 0 ? d_at(L) : -1;
+  const int dr = R < n ? d_at(R) : -1;
+  const int i = dr > dl ? R : L + 1;  // left child of R's node, else right child of L's
+  const bool leaf_l = g == L + 1, leaf_r = g + 1 == R;
+  pn[i] = uint8_t(D);
+  l8[i] = leaf_l;
+  r8[i] = leaf_r;
+  lcs[i] = g;
+  if (!leaf_l) par[g] = i;
+  if (!leaf_r) par[g + 1] = i;
+  if (EDGES) {
+    const int pd = max(dl, dr);
+    const int pp = pd == root_true_delta ? root_prefix : pd;
+    ec[i] = D / 3 - pp / 3;
+  }
+}
+
 template <typename K, bool EDGES>
 __global__ void __launch_bounds__(kTreeThreads)
     k_radix_tree(const K* __restrict__ codes_all, SegTable seg, TileMap map,
                  const uint32_t* __restrict__ n_unique, int32_t* __restrict__ seg_err,
                  uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
                  uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
-                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
-  constexpr int NPT = kTreeNpt, HALO = kTreeHalo;
-  constexpr int WIN = kTreeTile + 2 * HALO;
-  __shared__ K s_win[WIN];
+                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
+                 uint32_t* __restrict__ far, uint32_t far_cap, uint32_t* __restrict__ far_n) {
+  using C = AnsvCfg<K>;
+  constexpr int NV = C::NV, VB = C::VB, NW = kTreeThreads / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  K* s_key = reinterpret_cast<K*>(smem_raw);                                   // [kAnsvWin + 1]
+  int32_t* s_last = reinterpret_cast<int32_t*>(smem_raw + C::kKeyBytes);       // [NV][kAnsvRow]
+  int32_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
+  int32_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
+  int32_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
+  uint8_t* s_e = reinterpret_cast<uint8_t*>(s_rp + kTreeTile);                 // [kAnsvWin]
+
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
   const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
@@ -315,35 +433,169 @@ __global__ void __launch_bounds__(kTreeThreads)
   }
   const uint32_t sb = seg_begin(seg, c);
   const K* codes = codes_all + sb;
-  const int n = int(nu - 1);
-  const int base = int(blockIdx.x - first) * kTreeTile;
-  if (base >= n) return;
-  const int wlo = base - HALO;
-  for (int j = threadIdx.x; j < WIN; j += kTreeThreads) {
-    const int g = wlo + j;
-    s_win[j] = (g >= 0 && g <= n) ? codes[g] : K(0);
-  }
-  __syncthreads();
-  const KeyWindow<K> key{codes, s_win, wlo, WIN};
-  int root_true_delta = 0, root_prefix = 0;
-  if (EDGES) {
-    root_true_delta = delta(codes[0], codes[n]);
-    root_prefix = delta(codes[0], codes[n - 1]);
-  }
+  const int n = int(nu - 1);  // gaps (= nodes); keys are [0, n]
+  const int g0 = int(blockIdx.x - first) * int(kTreeTile);
+  if (g0 >= n) return;
+  const int wlo = g0 - kAnsvHalo * 32;  // first gap of the window
   uint8_t* pn = prefix_n + sb;
   uint8_t* l8 = hl + sb;
   uint8_t* r8 = hr + sb;
   int32_t* lcs = lc + sb;
   int32_t* par = parents + sb;
-#pragma unroll 1
-  for (int q = 0; q < NPT; ++q) {
-    const int i = base + q * kTreeThreads + int(threadIdx.x);
-    if (i >= n) break;
-    const BrtNode r = brt_node<K>(i, n, key);
-    write_node<K>(i, n, key, r, pn, l8, r8, lcs, par);
-    if (EDGES)
-      edge_count[sb + i] =
-          i > 0 ? fused_edge_count<K>(i, n, key, r, root_true_delta, root_prefix) : 0;
+
+  int root_true_delta = 0, root_prefix = 0;
+  if (EDGES) {
+    root_true_delta = delta(codes[0], codes[n]);
+    root_prefix = delta(codes[0], codes[n - 1]);
+  }
+  if (blockIdx.x == first && threadIdx.x == 0) {  // node 0, the reference's way
+    const GlobalKeys<K> gk{codes};
+    const BrtNode r = brt_node<K>(0, n, gk);
+    write_node<K>(0, n, gk, r, pn, l8, r8, lcs, par);
+    if (EDGES) edge_count[sb] = 0;
+  }
+
+  for (int j = threadIdx.x; j <= kAnsvWin; j += kTreeThreads) {
+    const int k = wlo + j;
+    s_key[j] = (k >= 0 && k <= n) ? codes[k] : K(0);
+  }
+  __syncthreads();
+
+  // phase A: per chunk, E, the nearest smaller inside the chunk, and the
+  // chunk's summaries (last / first position with E below each value)
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  for (int ch = int(warp); ch < kAnsvChunks; ch += NW) {
+    const int w = ch * 32 + int(lane);  // window index of this lane's gap
+    const int g = wlo + w;
+    const bool real = g >= 0 && g < n;
+    const int e = real ? max(delta(s_key[w], s_key[w + 1]) + 1, 0) : 0;
+    s_e[w] = uint8_t(e);
+    uint32_t lt = 0, eq = 0xffffffffu;      // lanes with E below mine
+    uint32_t lt0 = 0, eq0 = 0xffffffffu;    // lanes with E below v = lane
+    uint32_t lt1 = 0, eq1 = 0xffffffffu;    // lanes with E below v = lane + 32
+#pragma unroll
+    for (int bt = VB - 1; bt >= 0; --bt) {
+      const uint32_t B = __ballot_sync(0xffffffffu, (e >> bt) & 1);
+      if ((e >> bt) & 1) { lt |= eq & ~B; eq &= B; } else { eq &= ~B; }
+      const int v0 = int(lane);
+      if ((v0 >> bt) & 1) { lt0 |= eq0 & ~B; eq0 &= B; } else { eq0 &= ~B; }
+      if (NV > 32) {
+        const int v1 = int(lane) + 32;
+        if ((v1 >> bt) & 1) { lt1 |= eq1 & ~B; eq1 &= B; } else { eq1 &= ~B; }
+      }
+    }
+    const int cbase = wlo + ch * 32;
+    if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
+      const int tg = (ch - kAnsvHalo) * 32 + int(lane);
+      const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
+      s_lp[tg] = lm ? cbase + 31 - __clz(lm) : kAnsvNone;
+      s_rp[tg] = rm ? cbase + __ffs(rm) - 1 : kAnsvNoneR;
+    }
+    s_last[int(lane) * kAnsvRow + ch] = lt0 ? cbase + 31 - __clz(lt0) : kAnsvNone;
+    s_first[int(lane) * kAnsvRow + ch] = lt0 ? cbase + __ffs(lt0) - 1 : kAnsvNoneR;
+    if (NV > 32) {
+      s_last[(int(lane) + 32) * kAnsvRow + ch] = lt1 ? cbase + 31 - __clz(lt1) : kAnsvNone;
+      s_first[(int(lane) + 32) * kAnsvRow + ch] = lt1 ? cbase + __ffs(lt1) - 1 : kAnsvNoneR;
+    }
+  }
+  __syncthreads();
+
+  // phase B: exclusive prefix maximum of every value's "last" row and
+  // exclusive suffix minimum of its "first" row, over the window's chunks
+  for (int sq = int(warp); sq < 2 * NV; sq += NW) {
+    const bool left = sq < NV;
+    int32_t* row = left ? s_last + sq * kAnsvRow : s_first + (sq - NV) * kAnsvRow;
+    if (left) {
+      int carry = kAnsvNone;
+      for (int b0 = 0; b0 < kAnsvChunks; b0 += 32) {
+        const int ci = b0 + int(lane);
+        int x = ci < kAnsvChunks ? row[ci] : kAnsvNone;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, x, d);
+          if (int(lane) >= d) x = max(x, y);
+        }
+        int ex = __shfl_up_sync(0xffffffffu, x, 1);
+        if (lane == 0) ex = kAnsvNone;
+        if (ci < kAnsvChunks) row[ci] = max(ex, carry);
+        carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
+      }
+    } else {
+      int carry = kAnsvNoneR;
+      for (int b0 = ((kAnsvChunks - 1) / 32) * 32; b0 >= 0; b0 -= 32) {
+        const int ci = b0 + int(lane);
+        int x = ci < kAnsvChunks ? row[ci] : kAnsvNoneR;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_down_sync(0xffffffffu, x, d);
+          if (int(lane) + d < 32) x = min(x, y);
+        }
+        int ex = __shfl_down_sync(0xffffffffu, x, 1);
+        if (lane == 31) ex = kAnsvNoneR;
+        if (ci < kAnsvChunks) row[ci] = min(ex, carry);
+        carry = min(carry, __shfl_sync(0xffffffffu, x, 0));
+      }
+    }
+  }
+  __syncthreads();
+
+  // phase C: every gap of the tile writes its node; a gap whose nearest
+  // smaller gap lies beyond the window goes to the far-search list
+  const int wend = wlo + kAnsvWin - 1;  // last gap of the window
+  auto d_at = [&](int p) -> int {       // D of gap p in [0, n)
+    return (p >= wlo && p <= wend) ? int(s_e[p - wlo]) - 1 : delta(codes[p], codes[p + 1]);
+  };
+  for (int tg = int(threadIdx.x); tg < int(kTreeTile); tg += kTreeThreads) {
+    const int g = g0 + tg;
+    if (g >= n) break;
+    const int ch = kAnsvHalo + tg / 32;
+    const int e = s_e[g - wlo];
+    int L = s_lp[tg];
+    if (L == kAnsvNone) L = s_last[e * kAnsvRow + ch];
+    int R = s_rp[tg];
+    if (R == kAnsvNoneR) R = s_first[e * kAnsvRow + ch];
+    if (L == kAnsvNone || R == kAnsvNoneR) {
+      const uint32_t slot = atomicAdd(far_n, 1u);
+      if (slot < far_cap) {
+        far[2 * slot] = sb + uint32_t(g);
+        far[2 * slot + 1] = c;
+      }
+      continue;
+    }
+    write_gap_node<K, EDGES>(g, n, e - 1, max(L, -1), min(R, n), d_at, root_true_delta,
+                             root_prefix, pn, l8, r8, lcs, par,
+                             EDGES ? edge_count + sb : nullptr);
+  }
+}
+
+// The far-search list: one warp per listed gap finds both nearest smaller
+// gaps in global memory and writes the gap's node.
+template <typename K, bool EDGES>
+__global__ void __launch_bounds__(256)
+    k_radix_tree_far(const K* __restrict__ codes_all, SegTable seg,
+                     const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ far,
+                     const uint32_t* __restrict__ far_n, uint32_t far_cap,
+                     uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
+                     uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
+                     int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
+  const uint32_t count = min(*far_n, far_cap);
+  const uint32_t warps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w < count; w += warps) {
+    const uint32_t c = far[2 * w + 1];
+    const uint32_t sb = seg_begin(seg, c);
+    const int n = int(n_unique[c]) - 1;
+    const int g = int(far[2 * w] - sb);
+    const K* codes = codes_all + sb;
+    const int D = delta(codes[g], codes[g + 1]);
+    const int L = coop_first_key<K>(codes, g, D) - 1;
+    const int R = coop_last_key<K>(codes, n, g, D);
+    if (lane_id() == 0) {
+      auto d_at = [&](int p) -> int { return delta(codes[p], codes[p + 1]); };
+      const int rtd = EDGES ? delta(codes[0], codes[n]) : 0;
+      const int rp = EDGES ? delta(codes[0], codes[n - 1]) : 0;
+      write_gap_node<K, EDGES>(g, n, D, L, R, d_at, rtd, rp, prefix_n + sb, hl + sb, hr + sb,
+                               lc + sb, parents + sb, EDGES ? edge_count + sb : nullptr);
+    }
   }
 }
 
@@ -646,14 +898,27 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
   const uint32_t tiles = pl.tree_map.n_tiles;
   if (!tiles) return cudaSuccess;
   const K* codes = static_cast<const K*>(b.keys);
-  if (edges)
-    k_radix_tree<K, true><<<tiles, kTreeThreads, 0, s>>>(
+  constexpr size_t smem = AnsvCfg<K>::kSmem;
+  cudaError_t e = cudaFuncSetAttribute(edges ? k_radix_tree<K, true> : k_radix_tree<K, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  uint32_t* far_n = sc.tile_ctr + kCtrTree;
+  const int far_blocks = std::max(1, sc.num_sms * 2);
+  if (edges) {
+    k_radix_tree<K, true><<<tiles, kTreeThreads, smem, s>>>(
         codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
-        b.parents, b.edge_count);
-  else
-    k_radix_tree<K, false><<<tiles, kTreeThreads, 0, s>>>(
+        b.parents, b.edge_count, sc.tree_far, sc.tree_far_cap, far_n);
+    k_radix_tree_far<K, true><<<far_blocks, 256, 0, s>>>(
+        codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
+        b.hr, b.lc, b.parents, b.edge_count);
+  } else {
+    k_radix_tree<K, false><<<tiles, kTreeThreads, smem, s>>>(
         codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
-        b.parents, nullptr);
+        b.parents, nullptr, sc.tree_far, sc.tree_far_cap, far_n);
+    k_radix_tree_far<K, false><<<far_blocks, 256, 0, s>>>(
+        codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
+        b.hr, b.lc, b.parents, nullptr);
+  }
   return cudaGetLastError();
 }
 
