@@ -271,7 +271,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   const size_t ghist_b = align(size_t(n_clouds) * b->passes * radix * 4);
   const size_t sdesc_b = align(size_t(b->passes) * b->sort_rows * radix * 4);
   const size_t udesc_b = align((size_t(b->unique_tiles) + 1) * 4);
-  const size_t cdesc_b = align(size_t(b->scan_tiles) * 4);
+  const size_t cdesc_b = align((size_t(b->scan_tiles) + 1) * 4);
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
   const size_t per_b = align(size_t(n_clouds) * 4);

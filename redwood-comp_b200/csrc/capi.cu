@@ -210,8 +210,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
   const size_t ghist_b = align(size_t(im->passes) * radix * 4);
   const size_t sdesc_b = align(size_t(im->passes) * (im->sort_tiles + 1) * radix * 4);
   const size_t udesc_b = align((size_t(rwt::div_up(n_input, rwt::kUniqueTile)) + 1) * 4);
-  const size_t cdesc_b = align(size_t(std::max(rwt::div_up(n_input, rwt::kScanTile),
-                                               rwt::div_up(n_input, rwt::kTreeTile))) * 4);
+  const size_t cdesc_b = align((size_t(rwt::div_up(n_input, rwt::kScanTile)) + 1) * 4);
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
   im->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b;

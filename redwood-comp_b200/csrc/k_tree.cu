@@ -628,86 +628,133 @@ __global__ void __launch_bounds__(256)
 // stage 6: exclusive scan of the edge counts
 // ---------------------------------------------------------------------------
 
+// Stage 6 in two launches (no serial chain between tiles): (1) every tile
+// sums its edge counts into E[tile]; the block that finishes last scans E
+// (E[tiles] = total) and writes each segment's node count; (2) every tile
+// writes its exclusive offsets from E[tile] - E[the segment's first tile].
+// Tiles past a segment's nodes (the tile map is sized by points) count zero.
+__device__ __forceinline__ bool scan_tile(const SegTable& seg, const TileMap& map,
+                                          const uint32_t* n_unique, uint32_t tile,
+                                          uint32_t* c, uint32_t* firstt, uint32_t* n,
+                                          uint32_t* j) {
+  *c = tile_segment(seg, map, tile, firstt);
+  const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + *c);
+  const bool valid = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, *c);
+  *n = valid ? nu - 1 : 0;
+  *j = tile - *firstt;
+  return *j < (*n + kScanTile - 1) / kScanTile;
+}
+
+__device__ __forceinline__ void scan_load(const int32_t* ec, uint32_t first, uint32_t n,
+                                          bool vec, int32_t (&v)[kScanKpt]) {
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < kScanKpt / 4; ++q) {
+      const int4 x = reinterpret_cast<const int4*>(ec + first)[q];
+      v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < kScanKpt; ++q) v[q] = first + q < n ? ec[first + q] : 0;
+  }
+}
+
 __global__ void __launch_bounds__(kScanThreads)
-    k_edge_scan(const int32_t* __restrict__ ec_all, int32_t* __restrict__ off_all,
-                SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
-                uint32_t* __restrict__ n_octree, uint32_t* __restrict__ desc,
-                uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
-  constexpr int KPT = kScanKpt, NW = kScanThreads / 32;
+    k_scan_reduce(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
+                  const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ n_octree,
+                  uint32_t* __restrict__ E, uint32_t* __restrict__ done) {
+  constexpr int NW = kScanThreads / 32;
   __shared__ uint32_t s_warp[NW + 1];
-  __shared__ uint32_t s_tile, s_excl;
-  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  while (true) {
-    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= map.n_tiles) break;
-    uint32_t firstt;
-    const uint32_t c = tile_segment(seg, map, tile, &firstt);
-    const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
-    const bool valid = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, c);
-    const uint32_t n = valid ? nu - 1 : 0;
-    const uint32_t n_tiles_c = (n + kScanTile - 1) / kScanTile;
-    const uint32_t j = tile - firstt;
-    if (j >= n_tiles_c) {  // beyond this segment's nodes (uniform across the CTA)
-      __syncthreads();
-      continue;
-    }
+  __shared__ bool s_last;
+  const uint32_t tile = blockIdx.x;
+  uint32_t c, firstt, n, j;
+  uint32_t local = 0;
+  if (scan_tile(seg, map, n_unique, tile, &c, &firstt, &n, &j)) {
     const uint32_t sb = seg_begin(seg, c);
-    const int32_t* ec = ec_all + sb;
-    int32_t* off = off_all + sb;
-    const uint32_t first = j * kScanTile + tid * KPT;
-    int32_t v[KPT];
-    uint32_t local = 0;
-    const bool vec = first + KPT <= n && ((sb & 3u) == 0);
-    if (vec) {
+    const uint32_t first = j * kScanTile + threadIdx.x * kScanKpt;
+    int32_t v[kScanKpt];
+    scan_load(ec_all + sb, first, n, first + kScanKpt <= n && (sb & 3u) == 0, v);
 #pragma unroll
-      for (int q = 0; q < KPT / 4; ++q) {
-        const int4 x = reinterpret_cast<const int4*>(ec + first)[q];
-        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
-      }
-    } else {
+    for (int q = 0; q < kScanKpt; ++q) local += uint32_t(v[q]);
+  }
+  local = warp_sum(local);
+  if (lane_id() == 0) s_warp[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < NW; ++w) t += s_warp[w];
+    E[tile] = t;
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  constexpr int R = 8;
+  const uint32_t tiles = gridDim.x;
+  uint32_t carry = 0;
+  for (uint32_t c0 = 0; c0 < tiles; c0 += kScanThreads * R) {
+    const uint32_t f = c0 + threadIdx.x * R;
+    uint32_t v[R], loc = 0;
 #pragma unroll
-      for (int q = 0; q < KPT; ++q) v[q] = first + q < n ? ec[first + q] : 0;
+    for (int r = 0; r < R; ++r) {
+      v[r] = f + r < tiles ? __ldcg(E + f + r) : 0u;
+      loc += v[r];
     }
-#pragma unroll
-    for (int q = 0; q < KPT; ++q) local += uint32_t(v[q]);
     uint32_t total;
-    const uint32_t ex = block_exclusive_scan<kScanThreads>(local, s_warp, &total);
-    if (warp == 0) {
-      uint32_t excl = 0;
-      if (j == 0) {
-        if (lane == 0) st_relaxed(desc + tile, kFlagInc | (total << 2));
-      } else {
-        if (lane == 0) st_relaxed(desc + tile, kFlagAgg | (total << 2));
-        excl = warp_lookback(desc, tile, st, kSiteScan, firstt);
-        if (lane == 0) st_relaxed(desc + tile, kFlagInc | ((excl + total) << 2));
-      }
-      if (lane == 0) {
-        s_excl = excl;
-        if (j == n_tiles_c - 1) n_octree[c] = excl + total;
-      }
-    }
-    __syncthreads();
-    uint32_t run = s_excl + ex;
-    if (vec) {
+    uint32_t run = carry + block_exclusive_scan<kScanThreads>(loc, s_warp, &total);
 #pragma unroll
-      for (int q = 0; q < KPT / 4; ++q) {
-        int4 x;
-        x.x = int32_t(run); run += uint32_t(v[4 * q]);
-        x.y = int32_t(run); run += uint32_t(v[4 * q + 1]);
-        x.z = int32_t(run); run += uint32_t(v[4 * q + 2]);
-        x.w = int32_t(run); run += uint32_t(v[4 * q + 3]);
-        reinterpret_cast<int4*>(off + first)[q] = x;
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < KPT; ++q) {
-        if (first + q < n) off[first + q] = int32_t(run);
-        run += uint32_t(v[q]);
-      }
+    for (int r = 0; r < R; ++r) {
+      if (f + r < tiles) E[f + r] = run;
+      run += v[r];
     }
-    __syncthreads();
+    carry += total;
+  }
+  if (threadIdx.x == 0) E[tiles] = carry;
+  __syncthreads();
+  for (uint32_t sg = threadIdx.x; sg < seg.count; sg += kScanThreads) {
+    const uint32_t t0 = map.toff ? map.toff[sg] : 0u;
+    const uint32_t t1 = map.toff ? map.toff[sg + 1] : tiles;
+    n_octree[sg] = (t1 < tiles ? E[t1] : carry) - (t0 < tiles ? E[t0] : carry);
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_write(const int32_t* __restrict__ ec_all, int32_t* __restrict__ off_all,
+                 SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
+                 const uint32_t* __restrict__ E) {
+  __shared__ uint32_t s_warp[kScanThreads / 32 + 1];
+  const uint32_t tile = blockIdx.x;
+  uint32_t c, firstt, n, j;
+  if (!scan_tile(seg, map, n_unique, tile, &c, &firstt, &n, &j)) return;  // whole CTA
+  const uint32_t sb = seg_begin(seg, c);
+  const uint32_t first = j * kScanTile + threadIdx.x * kScanKpt;
+  const bool vec = first + kScanKpt <= n && (sb & 3u) == 0;
+  int32_t v[kScanKpt];
+  scan_load(ec_all + sb, first, n, vec, v);
+  uint32_t local = 0;
+#pragma unroll
+  for (int q = 0; q < kScanKpt; ++q) local += uint32_t(v[q]);
+  uint32_t total;
+  uint32_t run = (E[tile] - E[firstt]) +
+                 block_exclusive_scan<kScanThreads>(local, s_warp, &total);
+  int32_t* off = off_all + sb;
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < kScanKpt / 4; ++q) {
+      int4 x;
+      x.x = int32_t(run); run += uint32_t(v[4 * q]);
+      x.y = int32_t(run); run += uint32_t(v[4 * q + 1]);
+      x.z = int32_t(run); run += uint32_t(v[4 * q + 2]);
+      x.w = int32_t(run); run += uint32_t(v[4 * q + 3]);
+      reinterpret_cast<int4*>(off + first)[q] = x;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < kScanKpt; ++q) {
+      if (first + q < n) off[first + q] = int32_t(run);
+      run += uint32_t(v[q]);
+    }
   }
 }
 
@@ -878,7 +925,6 @@ __global__ void __launch_bounds__(kOctThreads)
 
 namespace {
 
-int persistent_blocks(const Scratch& sc, int per_sm) { return sc.num_sms * per_sm; }
 
 template <typename K>
 cudaError_t unique_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
@@ -987,10 +1033,11 @@ cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
 cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
   const uint32_t tiles = pl.scan_map.n_tiles;
   if (!tiles) return cudaSuccess;
-  const int blocks = std::max(1, std::min<int>(tiles, persistent_blocks(sc, 8)));
-  k_edge_scan<<<blocks, kScanThreads, 0, s>>>(b.edge_count, b.edge_offset, pl.seg,
-                                              pl.scan_map, pl.n_unique, pl.n_octree,
-                                              sc.scan_desc, sc.tile_ctr + kCtrScan, sc.status);
+  k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(b.edge_count, pl.seg, pl.scan_map, pl.n_unique,
+                                               pl.n_octree, sc.scan_desc,
+                                               sc.tile_ctr + kCtrScan);
+  k_scan_write<<<tiles, kScanThreads, 0, s>>>(b.edge_count, b.edge_offset, pl.seg,
+                                              pl.scan_map, pl.n_unique, sc.scan_desc);
   return cudaGetLastError();
 }
 
