@@ -500,11 +500,11 @@ def main():
                         "gbs": round(gbs, 1) if gbs else None,
                         "frac": round(gbs / hbm, 3) if gbs else None}
     dom = max(kms, key=kms.get)
-    tt = traffic_table()
+    tt = traffic_table().get("entries", {})
     dom_traffic = None
     key = f"{a.dist}-{a.key_bits}-{dom}"
-    if key in tt:
-        dom_traffic = tt[key]
+    if key in tt and a.n == 1 << 24:  # captured at this size (profiles/ncu_traffic.json)
+        dom_traffic = tt[key]["traffic"]
     dom_gbs = stages[dom]["gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": hbm,
                 "unit": "GB/s", "frac": round(dom_gbs / hbm, 4) if dom_gbs else None,
