@@ -52,23 +52,29 @@ __device__ __forceinline__ uint32_t tile_heads(const K* __restrict__ sorted, uin
                                                K (&keys)[kUniqueKpt],
                                                uint32_t (&heads)[kUniqueKpt]) {
   const uint32_t lane = lane_id();
+  // every load first, so that all of them are in flight together
+#pragma unroll
+  for (int i = 0; i < kUniqueKpt; ++i) {
+    const uint32_t idx = wbase + 32u * i + lane;
+    keys[i] = idx < n ? sorted[idx] : K(0);
+  }
+  const K before = (lane == 0 && wbase > sb && wbase - 1 < n) ? sorted[wbase - 1] : K(0);
   K carry = K(0);
   uint32_t count = 0;
 #pragma unroll
   for (int i = 0; i < kUniqueKpt; ++i) {
     const uint32_t idx = wbase + 32u * i + lane;
-    const K k = idx < n ? sorted[idx] : K(0);
+    const K k = keys[i];
     K left = __shfl_up_sync(0xffffffffu, k, 1);
     if (lane == 0) {
       if (i == 0)
-        left = (wbase > sb && wbase - 1 < n) ? sorted[wbase - 1] : K(~k);
+        left = (wbase > sb && wbase - 1 < n) ? before : K(~k);
       else
         left = carry;
     }
     carry = __shfl_sync(0xffffffffu, k, 31);
     const bool head = idx < n && (idx == sb || k != left);
     heads[i] = __ballot_sync(0xffffffffu, head);
-    keys[i] = k;
     count += __popc(heads[i]);
   }
   return count;
@@ -824,10 +830,18 @@ __global__ void __launch_bounds__(kOctThreads)
   const int n = os.n;
   const uint32_t m = os.m;
   const int root_level = prefix_n[0] / 3;
-  const int base = int(blockIdx.x - first) * kOctTile;
-  for (int q = 0; q < kOctNpt; ++q) {
-    const int i = base + q * kOctThreads + int(threadIdx.x);
-    if (i >= n) break;
+  // a warp takes 32 consecutive nodes; their rows are one contiguous run
+  // (the offsets are an exclusive scan), written 32 rows at a time: the row
+  // of lane j belongs to the last lane whose first row is <= it (a lane with
+  // no rows shares its first row with the next lane, which is later)
+  const uint32_t lane = lane_id();
+  const int wnodes = (kOctThreads / 32) * kOctNpt;  // warp-groups per tile x 32
+  const int tile0 = int(blockIdx.x - first) * kOctTile;
+  for (int q = int(threadIdx.x >> 5); q < wnodes; q += kOctThreads / 32) {
+    const int i0 = tile0 + q * 32;
+    if (i0 >= n) break;
+    const int i = i0 + int(lane);
+    const bool valid = i < n;
     if (i == 0) {
       const size_t rm = size_t(os.row0) + m;
       int4* row = reinterpret_cast<int4*>(o.children + 8 * rm);
@@ -840,25 +854,36 @@ __global__ void __launch_bounds__(kOctThreads)
         o.corner[os.row0] = decode<K>(K(pre << (B - 3 * root_level)), min_coord, range);
         o.cell_size[os.row0] = range;
       }
-      continue;
     }
-    const int cnt = ec[i];
-    if (cnt <= 0) continue;
-    const int rbase = off[i];
-    const K code = codes[i];
-    const int li = prefix_n[i] / 3;
-    for (int k = 0; k < cnt; ++k) {
-      const int p = rbase + k;
-      if (uint32_t(p) >= m) break;  // rows of a consistent scan lie below m
+    const int cnt = (valid && i > 0) ? max(ec[i], 0) : 0;
+    const int off_l = valid ? off[i] : 0x7fffffff;
+    const K code = valid ? codes[i] : K(0);
+    const int li = valid ? prefix_n[i] / 3 : 0;
+    const int total = warp_sum(cnt);
+    if (total == 0) continue;
+    const int r0 = __shfl_sync(0xffffffffu, off_l, 0);
+    for (int t = 0; t < total; t += 32) {
+      const int p = r0 + t + int(lane);
+      int owner = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int o_off = __shfl_sync(0xffffffffu, off_l, owner + step);
+        if (owner + step < 32 && o_off <= p) owner += step;
+      }
+      const int o_off = __shfl_sync(0xffffffffu, off_l, owner);
+      const int o_li = __shfl_sync(0xffffffffu, li, owner);
+      const K o_code = __shfl_sync(0xffffffffu, code, owner);
+      if (t + int(lane) >= total || uint32_t(p) >= m) continue;
       const size_t rp = size_t(os.row0) + uint32_t(p);
-      const int level = li - k;
-      const K pre = code >> (B - 3 * level);
+      const int k = p - o_off;
+      const int level = o_li - k;
+      const K pre = o_code >> (B - 3 * level);
       o.corner[rp] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
       o.cell_size[rp] = __fdiv_rn(range, float(1 << (level - root_level)));
       int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       int32_t mask = 0;
       if (k > 0) {
-        const int slot = int((code >> (B - 3 * (level + 1))) & K(7));
+        const int slot = int((o_code >> (B - 3 * (level + 1))) & K(7));
         child[slot] = p - 1;
         mask = 1 << slot;
       }

@@ -175,3 +175,28 @@ def test_pipeline_with_learned_sort_matches_oracle(rw, oracle, fused, mode):
     # back to onesweep on the same scratch
     im.set_learned(None)
     assert_same(run_gpu(rw, pts, fused=fused, im=im), oracle.run(pts, key_bits=32), "onesweep")
+
+
+def test_trained_network_gains_over_sample_quantiles(rw):
+    """What the trained boundary MLP buys over the method without it (plain
+    sample quantiles of the same 64K-key sample): on held-out mixtures (seeds
+    the network never saw) its buckets are more even, both in spread (cv) and
+    in the fullest bucket.  (Sort speed is a separate matter: both sorts run
+    the same kernels, and bench.py reports their times.)"""
+    from redwood_comp_b200 import learned
+    L = rw.Learned(1 << 23)
+    if L.params is None:
+        pytest.skip("no trained table")
+    n = 1 << 23
+    mlp, sq = [], []
+    for seed in range(learned.EVAL_SEED0 + 100, learned.EVAL_SEED0 + 106):
+        keys, _ = learned.morton_keys(rw, learned.mixture_cloud(rw, n, seed), sorted_too=False)
+        mlp.append(learned.balance(L.bucket_counts(keys, rw.LEARNED_MLP)))
+        sq.append(learned.balance(L.bucket_counts(keys, rw.LEARNED_SAMPLE_QUANTILES)))
+    cv_m = np.mean([b["cv"] for b in mlp]); cv_s = np.mean([b["cv"] for b in sq])
+    mx_m = np.mean([b["max_over_mean"] for b in mlp])
+    mx_s = np.mean([b["max_over_mean"] for b in sq])
+    print(f"bucket cv: mlp {cv_m:.4f} vs sample quantiles {cv_s:.4f}; "
+          f"max/mean: mlp {mx_m:.3f} vs {mx_s:.3f}")
+    assert cv_m < 0.97 * cv_s
+    assert mx_m < mx_s
