@@ -192,6 +192,17 @@ typedef struct rw_tree_host_out {
 int rw_tree_run_host(rw_tree_app_data* app, rw_tree_im_storage* im,
                      const float* h_points, rw_tree_host_out* h_out,
                      rw_stream_t stream);
+/* rw_tree_run_host in two halves, for streaming many clouds: submit copies
+ * h_points in and enqueues the pipeline, without waiting; collect waits for
+ * that run's counts (rw_tree_pipeline_finish) and enqueues the copies of the
+ * requested outputs, without waiting for them (h_out is complete once
+ * `stream` has drained).  With two AppData/scratch pairs on two streams, a
+ * caller alternating submit(k) and collect(k-1) overlaps one cloud's copies
+ * back with the next cloud's copies in and its pipeline. */
+int rw_tree_host_submit(rw_tree_app_data* app, rw_tree_im_storage* im, const float* h_points,
+                        rw_stream_t stream);
+int rw_tree_host_collect(rw_tree_app_data* app, rw_tree_im_storage* im,
+                         rw_tree_host_out* h_out, rw_stream_t stream);
 
 /* Seeded synthetic point clouds, generated on the host.
  *   RW_GEN_APPDATA: AppData's own generator (app_data.hpp:32-39):

@@ -105,7 +105,7 @@ EXPORTS = (
     "rw_tree_sort_profile",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
     "rw_tree_learned_set_group", "rw_tree_im_storage_set_learned",
-    "rw_tree_im_storage_learned_stats",
+    "rw_tree_im_storage_learned_stats", "rw_tree_host_submit", "rw_tree_host_collect",
     "rw_tree_learned_sort", "rw_tree_learned_features", "rw_tree_learned_bucket_counts",
     "rw_tree_mlp_param_count", "rw_tree_mlp_grad", "rw_tree_mlp_adam", "rw_tree_mlp_forward",
 )
@@ -415,6 +415,31 @@ def run_host(app: AppData, im: ImStorage, h_points: np.ndarray,
         setattr(ho, name, a.ctypes.data)
     _check(lib().rw_tree_run_host(ctypes.byref(app.c), im.handle, pts.ctypes.data_as(_vp),
                                   ctypes.byref(ho), _stream_handle(stream)), "run_host")
+
+
+def _host_out(out):
+    ho = _HostOutC()
+    for name, arr in (out or {}).items():
+        a = arr if isinstance(arr, np.ndarray) else arr.numpy()
+        setattr(ho, name, a.ctypes.data)
+    return ho
+
+
+def host_submit(app: AppData, im: ImStorage, h_points: np.ndarray, stream=None) -> None:
+    """Copies the (pinned) host points in and enqueues the pipeline, without
+    waiting (rw_tree_host_submit).  h_points must stay alive until `stream`
+    has drained."""
+    _check(lib().rw_tree_host_submit(ctypes.byref(app.c), im.handle,
+                                     h_points.ctypes.data_as(_vp), _stream_handle(stream)),
+           "host_submit")
+
+
+def host_collect(app: AppData, im: ImStorage, out: Optional[dict] = None, stream=None) -> None:
+    """Waits for the submitted run's counts and enqueues the copies of `out`'s
+    fields (rw_tree_host_collect); they are complete once `stream` has drained."""
+    ho = _host_out(out)
+    _check(lib().rw_tree_host_collect(ctypes.byref(app.c), im.handle, ctypes.byref(ho),
+                                      _stream_handle(stream)), "host_collect")
 
 
 class Batch:

@@ -555,17 +555,21 @@ int rw_tree_pipeline_finish(rw_tree_app_data* app, rw_tree_im_storage* im,
   return RW_OK;
 }
 
-int rw_tree_run_host(rw_tree_app_data* app, rw_tree_im_storage* im,
-                     const float* h_points, rw_tree_host_out* h_out,
-                     rw_stream_t stream) {
+int rw_tree_host_submit(rw_tree_app_data* app, rw_tree_im_storage* im, const float* h_points,
+                        rw_stream_t stream) {
   if (!h_points) return RW_ERR_ARG;
   if (int rc = check(app, im, kPoints | kKeys | kAlt | kBrt | kEdge | kOct)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   RW_CUDA(cudaMemcpyAsync(app->u_input_points, h_points, size_t(16) * app->n_input,
                           cudaMemcpyHostToDevice, s));
-  if (int rc = rw_tree_pipeline_enqueue(app, im, stream)) return rc;
+  return rw_tree_pipeline_enqueue(app, im, stream);
+}
+
+int rw_tree_host_collect(rw_tree_app_data* app, rw_tree_im_storage* im,
+                         rw_tree_host_out* h_out, rw_stream_t stream) {
   if (int rc = rw_tree_pipeline_finish(app, im, stream)) return rc;
   if (!h_out) return RW_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const size_t ks = key_size(app->key_bits);
   const size_t n = app->n_input, u = app->n_unique, b = app->n_brt_nodes,
                m = app->n_octree_nodes;
@@ -587,7 +591,15 @@ int rw_tree_run_host(rw_tree_app_data* app, rw_tree_im_storage* im,
   RW_CUDA(d2h(h_out->cell_size, app->oct_cell_size, 4 * m));
   RW_CUDA(d2h(h_out->child_node_mask, app->oct_child_node_mask, 4 * m));
   RW_CUDA(d2h(h_out->child_leaf_mask, app->oct_child_leaf_mask, 4 * m));
-  RW_CUDA(cudaStreamSynchronize(s));
+  return RW_OK;
+}
+
+int rw_tree_run_host(rw_tree_app_data* app, rw_tree_im_storage* im,
+                     const float* h_points, rw_tree_host_out* h_out,
+                     rw_stream_t stream) {
+  if (int rc = rw_tree_host_submit(app, im, h_points, stream)) return rc;
+  if (int rc = rw_tree_host_collect(app, im, h_out, stream)) return rc;
+  RW_CUDA(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
   return RW_OK;
 }
 
