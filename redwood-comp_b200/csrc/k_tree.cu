@@ -309,10 +309,11 @@ struct GlobalKeys {
 // comparison of E = D + 1 (0 marks the walls at -1 and n) gives every lane
 // the lanes with a smaller value, hence the nearest smaller in the chunk, and
 // every value v the last / first position in the chunk below v.  Across the
-// tile and a halo of kAnsvHalo chunks on either side, a prefix maximum and a
-// suffix minimum of those summaries answer the rest; a gap whose nearest
-// smaller lies beyond the halo (a node near the top of the tree) searches the
-// keys in global memory.
+// tile and a halo of kAnsvHalo chunks on either side, per-value bitmasks of
+// the chunks whose minimum lies below v find the nearest such chunk in one
+// clz / ffs, and its summary gives the answer; a gap whose nearest smaller
+// lies beyond the halo (a node near the top of the tree) goes to a list that a
+// second kernel resolves with warp-cooperative searches of the keys.
 constexpr int kAnsvHalo = 8;                                        // chunks per side
 constexpr int kAnsvChunks = int(kTreeTile) / 32 + 2 * kAnsvHalo;   // chunks per window
 constexpr int kAnsvWin = kAnsvChunks * 32;                           // gaps per window
@@ -325,8 +326,10 @@ struct AnsvCfg {
   static constexpr int NV = sizeof(K) == 4 ? 32 : 64;  // values of E
   static constexpr int VB = sizeof(K) == 4 ? 5 : 6;    // bits of E
   static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
+  static constexpr int MW = (kAnsvChunks + 31) / 32;  // mask words per value
   static constexpr size_t kSmem = kKeyBytes + 2 * size_t(NV) * kAnsvRow * 4 +
-                                  2 * size_t(kTreeTile) * 4 + size_t(kAnsvWin);
+                                  2 * size_t(kTreeTile) * 4 + size_t(NV) * MW * 4 +
+                                  size_t(kAnsvWin) + size_t(kAnsvChunks);
 };
 
 // Warp-cooperative searches for the nearest smaller gap of gap g beyond any
@@ -428,7 +431,9 @@ __global__ void __launch_bounds__(kTreeThreads)
   int32_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
   int32_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
   int32_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
-  uint8_t* s_e = reinterpret_cast<uint8_t*>(s_rp + kTreeTile);                 // [kAnsvWin]
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_rp + kTreeTile);            // [NV][MW]
+  uint8_t* s_e = reinterpret_cast<uint8_t*>(s_mask + NV * C::MW);              // [kAnsvWin]
+  uint8_t* s_cmin = s_e + kAnsvWin;                                            // [kAnsvChunks]
 
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
@@ -476,6 +481,8 @@ __global__ void __launch_bounds__(kTreeThreads)
     const bool real = g >= 0 && g < n;
     const int e = real ? max(delta(s_key[w], s_key[w + 1]) + 1, 0) : 0;
     s_e[w] = uint8_t(e);
+    const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e));
+    if (lane == 0) s_cmin[ch] = uint8_t(cmin);
     uint32_t lt = 0, eq = 0xffffffffu;      // lanes with E below mine
     uint32_t lt0 = 0, eq0 = 0xffffffffu;    // lanes with E below v = lane
     uint32_t lt1 = 0, eq1 = 0xffffffffu;    // lanes with E below v = lane + 32
@@ -506,41 +513,14 @@ __global__ void __launch_bounds__(kTreeThreads)
   }
   __syncthreads();
 
-  // phase B: exclusive prefix maximum of every value's "last" row and
-  // exclusive suffix minimum of its "first" row, over the window's chunks
-  for (int sq = int(warp); sq < 2 * NV; sq += NW) {
-    const bool left = sq < NV;
-    int32_t* row = left ? s_last + sq * kAnsvRow : s_first + (sq - NV) * kAnsvRow;
-    if (left) {
-      int carry = kAnsvNone;
-      for (int b0 = 0; b0 < kAnsvChunks; b0 += 32) {
-        const int ci = b0 + int(lane);
-        int x = ci < kAnsvChunks ? row[ci] : kAnsvNone;
+  // phase B: for every value v, a bitmask of the window's chunks whose
+  // minimum lies below v (bit c of word c / 32)
+  for (int v = int(warp); v < NV; v += NW) {
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, x, d);
-          if (int(lane) >= d) x = max(x, y);
-        }
-        int ex = __shfl_up_sync(0xffffffffu, x, 1);
-        if (lane == 0) ex = kAnsvNone;
-        if (ci < kAnsvChunks) row[ci] = max(ex, carry);
-        carry = max(carry, __shfl_sync(0xffffffffu, x, 31));
-      }
-    } else {
-      int carry = kAnsvNoneR;
-      for (int b0 = ((kAnsvChunks - 1) / 32) * 32; b0 >= 0; b0 -= 32) {
-        const int ci = b0 + int(lane);
-        int x = ci < kAnsvChunks ? row[ci] : kAnsvNoneR;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int y = __shfl_down_sync(0xffffffffu, x, d);
-          if (int(lane) + d < 32) x = min(x, y);
-        }
-        int ex = __shfl_down_sync(0xffffffffu, x, 1);
-        if (lane == 31) ex = kAnsvNoneR;
-        if (ci < kAnsvChunks) row[ci] = min(ex, carry);
-        carry = min(carry, __shfl_sync(0xffffffffu, x, 0));
-      }
+    for (int wd = 0; wd < C::MW; ++wd) {
+      const int cidx = wd * 32 + int(lane);
+      const uint32_t bits = __ballot_sync(0xffffffffu, cidx < kAnsvChunks && int(s_cmin[cidx]) < v);
+      if (lane == 0) s_mask[v * C::MW + wd] = bits;
     }
   }
   __syncthreads();
@@ -556,10 +536,30 @@ __global__ void __launch_bounds__(kTreeThreads)
     if (g >= n) break;
     const int ch = kAnsvHalo + tg / 32;
     const int e = s_e[g - wlo];
+    // not inside its own chunk: the nearest chunk on that side whose minimum
+    // is below e holds the answer in its summary
     int L = s_lp[tg];
-    if (L == kAnsvNone) L = s_last[e * kAnsvRow + ch];
+    if (L == kAnsvNone) {
+      for (int wd = (ch - 1) >> 5; wd >= 0; --wd) {
+        uint32_t bits = s_mask[e * C::MW + wd];
+        if (wd == (ch - 1) >> 5) bits &= 0xffffffffu >> (31 - ((ch - 1) & 31));
+        if (bits) {
+          L = s_last[e * kAnsvRow + wd * 32 + 31 - __clz(bits)];
+          break;
+        }
+      }
+    }
     int R = s_rp[tg];
-    if (R == kAnsvNoneR) R = s_first[e * kAnsvRow + ch];
+    if (R == kAnsvNoneR) {
+      for (int wd = (ch + 1) >> 5; wd < C::MW; ++wd) {
+        uint32_t bits = s_mask[e * C::MW + wd];
+        if (wd == (ch + 1) >> 5) bits &= 0xffffffffu << ((ch + 1) & 31);
+        if (bits) {
+          R = s_first[e * kAnsvRow + wd * 32 + __ffs(bits) - 1];
+          break;
+        }
+      }
+    }
     if (L == kAnsvNone || R == kAnsvNoneR) {
       const uint32_t slot = atomicAdd(far_n, 1u);
       if (slot < far_cap) {
