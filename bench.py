@@ -314,6 +314,85 @@ def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
     return info
 
 
+def measure_combined(rw, a, n_clouds=64, lo=1 << 20, hi=8 << 20, seed=880_001):
+    """The batched pipeline on 64 large clouds (sizes log-uniform in [1M, 8M],
+    Gaussian mixtures with 8-64 components, 64-bit keys) against the plain
+    pipeline run once per cloud; every cloud's outputs compared on the device
+    with its plain run.  (Stage 2 here is the onesweep sort: the learned-CDF
+    sort serves 32-bit keys.)"""
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = [int(np.exp(rng.uniform(np.log(lo), np.log(hi)))) for _ in range(n_clouds)]
+    clouds = [rw.generate_points(nc, rw.GEN_GAUSSIAN_MIXTURE, seed + c,
+                                 n_components=int(8 + (seed + c) * 2654435761 % 57),
+                                 sigma_lo=4.0, sigma_hi=40.0)
+              for c, nc in enumerate(sizes)]
+    total = int(sum(sizes))
+    ratio = 1.0
+    batch = rw.Batch(clouds, 64, octree_ratio=ratio)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        batch.run(graph=True)
+    torch.cuda.synchronize()
+    reps = 3
+    e0.record(s)
+    for _ in range(reps):
+        batch.enqueue(graph=True)
+    e1.record(s)
+    batch.finish()
+    batch_ms = e0.elapsed_time(e1) / reps
+    failed = int((batch.status != 0).sum())
+    # plain: one AppData/scratch per cloud, launches back to back
+    im = rw.ImStorage(max(sizes), 64)
+    apps = [rw.AppData(nc, 64, points=cl, octree_ratio=ratio) for nc, cl in zip(sizes, clouds)]
+    del clouds
+
+    def plain_once():
+        for app in apps:
+            rw.pipeline_enqueue(app, im)
+        rw.pipeline_finish(apps[-1], im)
+
+    plain_once()
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(reps):
+        plain_once()
+    e1.record(s)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / reps
+    mism = 0
+    for c, app in enumerate(apps):  # every cloud against its own plain run
+        rw.run_pipeline(app, im)
+        p0 = int(batch.point_offsets[c])
+        r0 = int(batch.octree_offsets[c])
+        u, m = app.get_n_unique(), app.get_n_octree_nodes()
+        same = int(batch.n_unique[c]) == u and int(batch.n_octree_nodes[c]) == m
+        pairs = [(batch.morton_keys_alt[p0:p0 + app.n_input], app.u_morton_keys_alt),
+                 (batch.morton_keys[p0:p0 + u], app.u_morton_keys[:u])]
+        for bf, af in (("prefix_n", "brt_prefix_n"), ("has_leaf_left", "brt_has_leaf_left"),
+                       ("has_leaf_right", "brt_has_leaf_right"), ("left_child", "brt_left_child"),
+                       ("parents", "brt_parents"), ("edge_count", "u_edge_count"),
+                       ("edge_offset", "u_edge_offset")):
+            pairs.append((getattr(batch, bf)[p0:p0 + u - 1], getattr(app, af)[:u - 1]))
+        for bf, af in (("children", "oct_children"), ("corner", "oct_corner"),
+                       ("cell_size", "oct_cell_size"), ("child_node_mask", "oct_child_node_mask"),
+                       ("child_leaf_mask", "oct_child_leaf_mask")):
+            pairs.append((getattr(batch, bf)[r0:r0 + m], getattr(app, af)[:m]))
+        mism += int(not same or not all(torch.equal(x, y) for x, y in pairs))
+    info = {
+        "workload": f"combined: {n_clouds} clouds, sizes log-uniform in [1M, 8M] (total "
+                    f"{total:,} points), Gaussian mixtures with 8-64 components, 64-bit keys, "
+                    f"octree rows {ratio} per point; stage 2 onesweep (no 64-bit learned sort)",
+        "value": total / (batch_ms / 1e3), "unit": "points/s", "ms_per_batch": batch_ms,
+        "plain_per_cloud_value": total / (plain_ms / 1e3), "plain_per_cloud_ms": plain_ms,
+        "speedup_vs_plain": plain_ms / batch_ms, "clouds_failed": failed,
+        "clouds_compared_with_plain": n_clouds, "mismatched_clouds": mism, "graph": True,
+    }
+    batch.close()
+    return info
+
+
 LEARNED_SEED = 950_001  # held out: the boundary MLP trains on seeds 500,000-500,159
 
 
@@ -589,6 +668,8 @@ def main():
         forms = {"batched": measure_batch(rw, a)}
         torch.cuda.empty_cache()
         forms["learned"] = measure_learned(rw, a)
+        torch.cuda.empty_cache()
+        forms["combined"] = measure_combined(rw, a)
 
     if world > 1:
         dist.destroy_process_group()
