@@ -29,11 +29,11 @@ namespace rwt {
 // each CTA takes a contiguous run of tiles, so with HIST its shared-memory
 // histograms are flushed to the segment's global ones only when the segment
 // changes.  ghist: [segments][passes][RADIX].
-template <typename K, int D, bool HIST, bool ENCODE>
+template <typename K, int D, bool HIST, bool ENCODE, bool POW2>
 __global__ void __launch_bounds__(256)
     k_keys_pass(const float4* __restrict__ pts, K* __restrict__ keys, SegTable seg,
                 TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
-                uint32_t* __restrict__ ghist, int passes) {
+                float inv_range, uint32_t* __restrict__ ghist, int passes) {
   constexpr int RADIX = 1 << D;
   extern __shared__ uint32_t s_hist[];  // [passes][RADIX] when HIST
   const int nh = passes * RADIX;
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256)
       K k;
       if (ENCODE) {
         const float4 p = __ldcs(pts + i);
-        k = encode<K>(p.x, p.y, p.z, min_coord, range);
+        k = encode<K, POW2>(p.x, p.y, p.z, min_coord, range, inv_range);
         keys[i] = k;
       } else {
         k = keys[i];
@@ -298,13 +298,14 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
   const uint32_t grid = div_up(tiles, per);
   const size_t smem = hist ? size_t(sc.passes) * (1u << D) * 4 : 0;
   K* keys = static_cast<K*>(b.keys);
+  const float inv = pow2_reciprocal(b.range);
 #define RWT_KEYS_LAUNCH(H, E)                                                        \
   do {                                                                               \
-    auto kern = k_keys_pass<K, D, H, E>;                                             \
+    auto kern = inv != 0.0f ? k_keys_pass<K, D, H, E, true> : k_keys_pass<K, D, H, E, false>; \
     if (smem > 48 * 1024)                                                            \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
     kern<<<grid, 256, smem, s>>>(b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
-                                 b.range, sc.ghist, sc.passes);                      \
+                                 b.range, inv, sc.ghist, sc.passes);                 \
   } while (0)
   if (encode && hist) RWT_KEYS_LAUNCH(true, true);
   else if (encode) RWT_KEYS_LAUNCH(false, true);

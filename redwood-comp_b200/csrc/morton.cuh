@@ -72,22 +72,41 @@ struct KeyTraits<uint64_t> {
 // (c - min) / range * 2^axis_bits, truncated to unsigned, masked to the axis
 // width (func_morton.hpp:27-30).  Coordinates below min are outside the
 // reference's defined behaviour (its float->unsigned cast is undefined there).
-template <typename K>
-__device__ __forceinline__ uint32_t quantise(float c, float min_coord,
-                                             float range) {
+// With POW2 the caller has checked that range is a power of two (2^k with k
+// in [-126, 126]) and passes inv_range = 2^-k: (c - min) / range and
+// (c - min) * 2^-k are then both the correctly rounded value of the same real
+// number, so the product equals the IEEE quotient bit for bit.
+template <typename K, bool POW2 = false>
+__device__ __forceinline__ uint32_t quantise(float c, float min_coord, float range,
+                                             float inv_range = 0.0f) {
   constexpr float kScale = float(1u << KeyTraits<K>::kAxisBits);
-  const float q = __fmul_rn(__fdiv_rn(__fsub_rn(c, min_coord), range), kScale);
+  const float d = __fsub_rn(c, min_coord);
+  const float t = POW2 ? __fmul_rn(d, inv_range) : __fdiv_rn(d, range);
+  const float q = __fmul_rn(t, kScale);
   return __float2uint_rz(q) & ((1u << KeyTraits<K>::kAxisBits) - 1u);
 }
 
-template <typename K>
+template <typename K, bool POW2 = false>
 __device__ __forceinline__ K encode(float x, float y, float z, float min_coord,
-                                    float range) {
+                                    float range, float inv_range = 0.0f) {
   using T = KeyTraits<K>;
-  const K ix = T::spread(K(quantise<K>(x, min_coord, range)));
-  const K iy = T::spread(K(quantise<K>(y, min_coord, range)));
-  const K iz = T::spread(K(quantise<K>(z, min_coord, range)));
+  const K ix = T::spread(K(quantise<K, POW2>(x, min_coord, range, inv_range)));
+  const K iy = T::spread(K(quantise<K, POW2>(y, min_coord, range, inv_range)));
+  const K iz = T::spread(K(quantise<K, POW2>(z, min_coord, range, inv_range)));
   return ix | (iy << 1) | (iz << 2);
+}
+
+// 2^-k when range = 2^k (k in [-126, 126]), else 0 (host side).
+inline float pow2_reciprocal(float range) {
+  uint32_t b;
+  static_assert(sizeof(b) == sizeof(range), "float is 32 bits");
+  __builtin_memcpy(&b, &range, 4);
+  const uint32_t ex = (b >> 23) & 0xffu;
+  if ((b & 0x807fffffu) != 0 || ex < 1 || ex > 253) return 0.0f;
+  const uint32_t r = (254u - ex) << 23;
+  float out;
+  __builtin_memcpy(&out, &r, 4);
+  return out;
 }
 
 // morton32_to_xyz (func_morton.hpp:60-80): float(d) / scale * range + min,
@@ -100,9 +119,12 @@ __device__ __forceinline__ float4 decode(K code, float min_coord, float range) {
   const float fy = __uint2float_rn(uint32_t(T::gather(code >> 1)));
   const float fz = __uint2float_rn(uint32_t(T::gather(code >> 2)));
   float4 r;
-  r.x = __fadd_rn(__fmul_rn(__fdiv_rn(fx, kScale), range), min_coord);
-  r.y = __fadd_rn(__fmul_rn(__fdiv_rn(fy, kScale), range), min_coord);
-  r.z = __fadd_rn(__fmul_rn(__fdiv_rn(fz, kScale), range), min_coord);
+  // kScale is a power of two: dividing by it is multiplying by its exact
+  // reciprocal (the same correctly rounded value)
+  constexpr float kInv = 1.0f / kScale;
+  r.x = __fadd_rn(__fmul_rn(__fmul_rn(fx, kInv), range), min_coord);
+  r.y = __fadd_rn(__fmul_rn(__fmul_rn(fy, kInv), range), min_coord);
+  r.z = __fadd_rn(__fmul_rn(__fmul_rn(fz, kInv), range), min_coord);
   r.w = 1.0f;
   return r;
 }

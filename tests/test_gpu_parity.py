@@ -194,3 +194,22 @@ def test_every_sort_variant_is_exact(rw, oracle):
         im.set_sort_variant(v["index"])
         rw.run_pipeline(app, im)
         assert_same(app.results(), oracle.run(pts, key_bits=kb), f"variant {v}")
+
+
+@pytest.mark.parametrize("key_bits", [32, 64])
+@pytest.mark.parametrize("box", [(-3.5, 2048.0), (7.25, 1000.0), (0.0, 0.375)])
+def test_other_bounds(rw, oracle, key_bits, box):
+    """Quantisation against the oracle for bounds other than [0, 1024): a
+    power-of-two range (multiplication by the exact reciprocal) and ranges
+    that are not (IEEE division), with a nonzero minimum."""
+    mn, rg = box
+    n = 300_001
+    rng = np.random.default_rng(int(rg * 8) + key_bits)
+    pts = np.zeros((n, 4), np.float32)
+    pts[:, :3] = (mn + rng.random((n, 3)) * rg * 0.999).astype(np.float32)
+    pts[:, 3] = 1.0
+    app = rw.AppData(n, key_bits, points=pts, min_coord=mn, range_=rg)
+    im = rw.ImStorage(n, key_bits)
+    rw.run_pipeline(app, im)
+    want = oracle.run(pts, key_bits=key_bits, min_coord=mn, range_=rg)
+    assert_same(app.results(), want, f"box {box} key_bits {key_bits}")
