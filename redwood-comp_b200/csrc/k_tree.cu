@@ -39,12 +39,48 @@ namespace rwt {
 // stage 3: unique
 // ---------------------------------------------------------------------------
 
-// Stage 3 in two launches without a serial chain between tiles: (1) every
+// Exclusive scan of per-tile values E[0, tiles) in place (E[tiles] = total),
+// one block; then each segment's total (its tiles per the tile map) into
+// seg_total.  Between the per-tile count and the per-tile write launches of
+// stages 3 and 6.
+__global__ void __launch_bounds__(1024)
+    k_tile_scan(uint32_t* __restrict__ E, uint32_t tiles, SegTable seg, TileMap map,
+                uint32_t* __restrict__ seg_total) {
+  __shared__ uint32_t s_warp[33];
+  constexpr int R = 8;
+  uint32_t carry = 0;
+  for (uint32_t c0 = 0; c0 < tiles; c0 += 1024 * R) {
+    const uint32_t f = c0 + threadIdx.x * R;
+    uint32_t v[R], loc = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      v[r] = f + r < tiles ? E[f + r] : 0u;
+      loc += v[r];
+    }
+    uint32_t total;
+    uint32_t run = carry + block_exclusive_scan<1024>(loc, s_warp, &total);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (f + r < tiles) E[f + r] = run;
+      run += v[r];
+    }
+    carry += total;
+  }
+  if (threadIdx.x == 0) E[tiles] = carry;
+  __syncthreads();
+  for (uint32_t sg = threadIdx.x; sg < seg.count; sg += 1024) {
+    const uint32_t t0 = map.toff ? map.toff[sg] : 0u;
+    const uint32_t t1 = map.toff ? map.toff[sg + 1] : tiles;
+    seg_total[sg] = (t1 < tiles ? E[t1] : carry) - (t0 < tiles ? E[t0] : carry);
+  }
+}
+
+// Stage 3 in three launches without a serial chain between tiles: (1) every
 // tile counts its heads (a key is a head when it differs from its left
-// neighbour in the segment, or starts the segment) into E[tile]; the block
-// that finishes last turns E into its exclusive scan (E[tiles] = total) and
-// writes each segment's n_unique; (2) every tile compacts its heads to
-// segment begin + E[tile] - E[first tile of the segment].  Same result as
+// neighbour in the segment, or starts the segment) into E[tile]; (2) one block
+// turns E into its exclusive scan (E[tiles] = total) and writes each
+// segment's n_unique; (3) every tile compacts its heads to segment begin +
+// E[tile] - E[first tile of the segment].  Same result as
 // cu_dispatcher.cu:597-627 (a std::unique over the sorted keys).
 template <typename K>
 __device__ __forceinline__ uint32_t tile_heads(const K* __restrict__ sorted, uint32_t sb,
@@ -83,11 +119,9 @@ __device__ __forceinline__ uint32_t tile_heads(const K* __restrict__ sorted, uin
 template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
     k_unique_count(const K* __restrict__ sorted, SegTable seg, TileMap map,
-                   uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E,
-                   uint32_t* __restrict__ done) {
+                   uint32_t* __restrict__ E) {
   constexpr int NW = kUniqueThreads / 32;
-  __shared__ uint32_t s_warp[NW + 1];
-  __shared__ bool s_last;
+  __shared__ uint32_t s_warp[NW];
   const uint32_t tile = blockIdx.x, lane = lane_id(), warp = threadIdx.x >> 5;
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, tile, &first);
@@ -103,42 +137,6 @@ __global__ void __launch_bounds__(kUniqueThreads)
     uint32_t t = 0;
     for (int w = 0; w < NW; ++w) t += s_warp[w];
     E[tile] = t;
-    __threadfence();
-    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  // the last block: exclusive scan of E[0, tiles) in place, in chunks of
-  // kUniqueThreads * 8 (every other block's count is visible: each fenced
-  // its write before its increment of `done`)
-  __threadfence();
-  constexpr int R = 8;
-  const uint32_t tiles = gridDim.x;
-  uint32_t carry = 0;
-  for (uint32_t c0 = 0; c0 < tiles; c0 += kUniqueThreads * R) {
-    const uint32_t f = c0 + threadIdx.x * R;
-    uint32_t v[R], local = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      v[r] = f + r < tiles ? __ldcg(E + f + r) : 0u;
-      local += v[r];
-    }
-    uint32_t total;
-    uint32_t run = carry + block_exclusive_scan<kUniqueThreads>(local, s_warp, &total);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (f + r < tiles) E[f + r] = run;
-      run += v[r];
-    }
-    carry += total;
-  }
-  if (threadIdx.x == 0) E[tiles] = carry;
-  __syncthreads();
-  __threadfence_block();
-  for (uint32_t sg = threadIdx.x; sg < seg.count; sg += kUniqueThreads) {
-    const uint32_t t0 = map.toff ? map.toff[sg] : 0u;
-    const uint32_t t1 = map.toff ? map.toff[sg + 1] : tiles;
-    n_unique[sg] = (t1 < tiles ? E[t1] : carry) - (t0 < tiles ? E[t0] : carry);
   }
 }
 
@@ -634,10 +632,10 @@ __global__ void __launch_bounds__(256)
 // stage 6: exclusive scan of the edge counts
 // ---------------------------------------------------------------------------
 
-// Stage 6 in two launches (no serial chain between tiles): (1) every tile
-// sums its edge counts into E[tile]; the block that finishes last scans E
-// (E[tiles] = total) and writes each segment's node count; (2) every tile
-// writes its exclusive offsets from E[tile] - E[the segment's first tile].
+// Stage 6 in three launches (no serial chain between tiles): (1) every tile
+// sums its edge counts into E[tile]; (2) one block scans E (E[tiles] = total)
+// and writes each segment's node count; (3) every tile writes its exclusive
+// offsets from E[tile] - E[the segment's first tile].
 // Tiles past a segment's nodes (the tile map is sized by points) count zero.
 __device__ __forceinline__ bool scan_tile(const SegTable& seg, const TileMap& map,
                                           const uint32_t* n_unique, uint32_t tile,
@@ -667,11 +665,9 @@ __device__ __forceinline__ void scan_load(const int32_t* ec, uint32_t first, uin
 
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_reduce(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
-                  const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ n_octree,
-                  uint32_t* __restrict__ E, uint32_t* __restrict__ done) {
+                  const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E) {
   constexpr int NW = kScanThreads / 32;
-  __shared__ uint32_t s_warp[NW + 1];
-  __shared__ bool s_last;
+  __shared__ uint32_t s_warp[NW];
   const uint32_t tile = blockIdx.x;
   uint32_t c, firstt, n, j;
   uint32_t local = 0;
@@ -690,38 +686,6 @@ __global__ void __launch_bounds__(kScanThreads)
     uint32_t t = 0;
     for (int w = 0; w < NW; ++w) t += s_warp[w];
     E[tile] = t;
-    __threadfence();
-    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  constexpr int R = 8;
-  const uint32_t tiles = gridDim.x;
-  uint32_t carry = 0;
-  for (uint32_t c0 = 0; c0 < tiles; c0 += kScanThreads * R) {
-    const uint32_t f = c0 + threadIdx.x * R;
-    uint32_t v[R], loc = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      v[r] = f + r < tiles ? __ldcg(E + f + r) : 0u;
-      loc += v[r];
-    }
-    uint32_t total;
-    uint32_t run = carry + block_exclusive_scan<kScanThreads>(loc, s_warp, &total);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (f + r < tiles) E[f + r] = run;
-      run += v[r];
-    }
-    carry += total;
-  }
-  if (threadIdx.x == 0) E[tiles] = carry;
-  __syncthreads();
-  for (uint32_t sg = threadIdx.x; sg < seg.count; sg += kScanThreads) {
-    const uint32_t t0 = map.toff ? map.toff[sg] : 0u;
-    const uint32_t t1 = map.toff ? map.toff[sg + 1] : tiles;
-    n_octree[sg] = (t1 < tiles ? E[t1] : carry) - (t0 < tiles ? E[t0] : carry);
   }
 }
 
@@ -879,7 +843,9 @@ __global__ void __launch_bounds__(kOctThreads)
       const int level = o_li - k;
       const K pre = o_code >> (B - 3 * level);
       o.corner[rp] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
-      o.cell_size[rp] = __fdiv_rn(range, float(1 << (level - root_level)));
+      // range / 2^s, s = level - root_level in [0, 21]: the product with the
+      // exact reciprocal 2^-s is the same correctly rounded value
+      o.cell_size[rp] = __fmul_rn(range, __uint_as_float(uint32_t(127 - (level - root_level)) << 23));
       int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       int32_t mask = 0;
       if (k > 0) {
@@ -956,8 +922,9 @@ cudaError_t unique_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   const uint32_t tiles = pl.unique_map.n_tiles;
   if (!tiles) return cudaSuccess;
   const K* sorted = static_cast<const K*>(b.alt);
-  k_unique_count<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, pl.seg, pl.unique_map, pl.n_unique,
-                                                     sc.unique_desc, sc.tile_ctr + kCtrUnique);
+  k_unique_count<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, pl.seg, pl.unique_map,
+                                                     sc.unique_desc);
+  k_tile_scan<<<1, 1024, 0, s>>>(sc.unique_desc, tiles, pl.seg, pl.unique_map, pl.n_unique);
   k_unique_write<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, static_cast<K*>(b.keys), pl.seg,
                                                      pl.unique_map, sc.unique_desc);
   return cudaGetLastError();
@@ -1059,8 +1026,8 @@ cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, c
   const uint32_t tiles = pl.scan_map.n_tiles;
   if (!tiles) return cudaSuccess;
   k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(b.edge_count, pl.seg, pl.scan_map, pl.n_unique,
-                                               pl.n_octree, sc.scan_desc,
-                                               sc.tile_ctr + kCtrScan);
+                                               sc.scan_desc);
+  k_tile_scan<<<1, 1024, 0, s>>>(sc.scan_desc, tiles, pl.seg, pl.scan_map, pl.n_octree);
   k_scan_write<<<tiles, kScanThreads, 0, s>>>(b.edge_count, b.edge_offset, pl.seg,
                                               pl.scan_map, pl.n_unique, sc.scan_desc);
   return cudaGetLastError();
