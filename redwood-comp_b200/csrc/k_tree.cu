@@ -481,13 +481,14 @@ __global__ void __launch_bounds__(kTreeThreads)
     s_e[w] = uint8_t(e);
     const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e));
     if (lane == 0) s_cmin[ch] = uint8_t(cmin);
-    uint32_t lt = 0, eq = 0xffffffffu;      // lanes with E below mine
+    // bit-serial comparison of every lane's E against v = lane (and lane + 32
+    // for 64-bit keys): lane v ends with the lanes whose E is below v; the
+    // lanes below my own value are then lane e's result
     uint32_t lt0 = 0, eq0 = 0xffffffffu;    // lanes with E below v = lane
     uint32_t lt1 = 0, eq1 = 0xffffffffu;    // lanes with E below v = lane + 32
 #pragma unroll
     for (int bt = VB - 1; bt >= 0; --bt) {
       const uint32_t B = __ballot_sync(0xffffffffu, (e >> bt) & 1);
-      if ((e >> bt) & 1) { lt |= eq & ~B; eq &= B; } else { eq &= ~B; }
       const int v0 = int(lane);
       if ((v0 >> bt) & 1) { lt0 |= eq0 & ~B; eq0 &= B; } else { eq0 &= ~B; }
       if (NV > 32) {
@@ -495,6 +496,9 @@ __global__ void __launch_bounds__(kTreeThreads)
         if ((v1 >> bt) & 1) { lt1 |= eq1 & ~B; eq1 &= B; } else { eq1 &= ~B; }
       }
     }
+    const uint32_t from0 = __shfl_sync(0xffffffffu, lt0, e & 31);
+    const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1, e & 31) : 0u;
+    const uint32_t lt = (NV > 32 && e >= 32) ? from1 : from0;
     const int cbase = wlo + ch * 32;
     if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
       const int tg = (ch - kAnsvHalo) * 32 + int(lane);
