@@ -473,44 +473,61 @@ __global__ void __launch_bounds__(kTreeThreads)
   // phase A: per chunk, E, the nearest smaller inside the chunk, and the
   // chunk's summaries (last / first position with E below each value)
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  for (int ch = int(warp); ch < kAnsvChunks; ch += NW) {
-    const int w = ch * 32 + int(lane);  // window index of this lane's gap
-    const int g = wlo + w;
-    const bool real = g >= 0 && g < n;
-    const int e = real ? max(delta(s_key[w], s_key[w + 1]) + 1, 0) : 0;
-    s_e[w] = uint8_t(e);
-    const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e));
-    if (lane == 0) s_cmin[ch] = uint8_t(cmin);
+  // two chunks at a time per warp, so that their ballot chains interleave
+  static_assert(kAnsvChunks % (2 * NW) == 0, "whole pairs of chunks per warp");
+  for (int ch0 = int(warp); ch0 < kAnsvChunks; ch0 += 2 * NW) {
+    int e[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int ch = ch0 + j * NW;
+      const int w = ch * 32 + int(lane);  // window index of this lane's gap
+      const int g = wlo + w;
+      const bool real = g >= 0 && g < n;
+      e[j] = real ? max(delta(s_key[w], s_key[w + 1]) + 1, 0) : 0;
+      s_e[w] = uint8_t(e[j]);
+      const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e[j]));
+      if (lane == 0) s_cmin[ch] = uint8_t(cmin);
+    }
     // bit-serial comparison of every lane's E against v = lane (and lane + 32
     // for 64-bit keys): lane v ends with the lanes whose E is below v; the
     // lanes below my own value are then lane e's result
-    uint32_t lt0 = 0, eq0 = 0xffffffffu;    // lanes with E below v = lane
-    uint32_t lt1 = 0, eq1 = 0xffffffffu;    // lanes with E below v = lane + 32
+    uint32_t lt0[2] = {0, 0}, eq0[2] = {0xffffffffu, 0xffffffffu};  // below v = lane
+    uint32_t lt1[2] = {0, 0}, eq1[2] = {0xffffffffu, 0xffffffffu};  // below v = lane + 32
 #pragma unroll
     for (int bt = VB - 1; bt >= 0; --bt) {
-      const uint32_t B = __ballot_sync(0xffffffffu, (e >> bt) & 1);
-      const int v0 = int(lane);
-      if ((v0 >> bt) & 1) { lt0 |= eq0 & ~B; eq0 &= B; } else { eq0 &= ~B; }
-      if (NV > 32) {
-        const int v1 = int(lane) + 32;
-        if ((v1 >> bt) & 1) { lt1 |= eq1 & ~B; eq1 &= B; } else { eq1 &= ~B; }
+      uint32_t B[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) B[j] = __ballot_sync(0xffffffffu, (e[j] >> bt) & 1);
+      const bool b0 = (int(lane) >> bt) & 1, b1 = ((int(lane) + 32) >> bt) & 1;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (b0) { lt0[j] |= eq0[j] & ~B[j]; eq0[j] &= B[j]; } else { eq0[j] &= ~B[j]; }
+        if (NV > 32) {
+          if (b1) { lt1[j] |= eq1[j] & ~B[j]; eq1[j] &= B[j]; } else { eq1[j] &= ~B[j]; }
+        }
       }
     }
-    const uint32_t from0 = __shfl_sync(0xffffffffu, lt0, e & 31);
-    const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1, e & 31) : 0u;
-    const uint32_t lt = (NV > 32 && e >= 32) ? from1 : from0;
-    const int cbase = wlo + ch * 32;
-    if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
-      const int tg = (ch - kAnsvHalo) * 32 + int(lane);
-      const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
-      s_lp[tg] = lm ? cbase + 31 - __clz(lm) : kAnsvNone;
-      s_rp[tg] = rm ? cbase + __ffs(rm) - 1 : kAnsvNoneR;
-    }
-    s_last[int(lane) * kAnsvRow + ch] = lt0 ? cbase + 31 - __clz(lt0) : kAnsvNone;
-    s_first[int(lane) * kAnsvRow + ch] = lt0 ? cbase + __ffs(lt0) - 1 : kAnsvNoneR;
-    if (NV > 32) {
-      s_last[(int(lane) + 32) * kAnsvRow + ch] = lt1 ? cbase + 31 - __clz(lt1) : kAnsvNone;
-      s_first[(int(lane) + 32) * kAnsvRow + ch] = lt1 ? cbase + __ffs(lt1) - 1 : kAnsvNoneR;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int ch = ch0 + j * NW;
+      const uint32_t from0 = __shfl_sync(0xffffffffu, lt0[j], e[j] & 31);
+      const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1[j], e[j] & 31) : 0u;
+      const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
+      const int cbase = wlo + ch * 32;
+      if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
+        const int tg = (ch - kAnsvHalo) * 32 + int(lane);
+        const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
+        s_lp[tg] = lm ? cbase + 31 - __clz(lm) : kAnsvNone;
+        s_rp[tg] = rm ? cbase + __ffs(rm) - 1 : kAnsvNoneR;
+      }
+      s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? cbase + 31 - __clz(lt0[j]) : kAnsvNone;
+      s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? cbase + __ffs(lt0[j]) - 1 : kAnsvNoneR;
+      if (NV > 32) {
+        s_last[(int(lane) + 32) * kAnsvRow + ch] =
+            lt1[j] ? cbase + 31 - __clz(lt1[j]) : kAnsvNone;
+        s_first[(int(lane) + 32) * kAnsvRow + ch] =
+            lt1[j] ? cbase + __ffs(lt1[j]) - 1 : kAnsvNoneR;
+      }
     }
   }
   __syncthreads();
