@@ -325,9 +325,8 @@ struct AnsvCfg {
   static constexpr int VB = sizeof(K) == 4 ? 5 : 6;    // bits of E
   static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
   static constexpr int MW = (kAnsvChunks + 31) / 32;  // mask words per value
-  static constexpr size_t kSmem = kKeyBytes + 2 * size_t(NV) * kAnsvRow * 4 +
-                                  2 * size_t(kTreeTile) * 4 + size_t(NV) * MW * 4 +
-                                  size_t(kAnsvWin) + size_t(kAnsvChunks);
+  static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 + 2 * size_t(NV) * kAnsvRow +
+                                  2 * size_t(kTreeTile) + size_t(kAnsvWin) + size_t(kAnsvChunks);
 };
 
 // Warp-cooperative searches for the nearest smaller gap of gap g beyond any
@@ -424,13 +423,14 @@ __global__ void __launch_bounds__(kTreeThreads)
   using C = AnsvCfg<K>;
   constexpr int NV = C::NV, VB = C::VB, NW = kTreeThreads / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // positions inside a chunk are kept as lane indices (0xff: none)
   K* s_key = reinterpret_cast<K*>(smem_raw);                                   // [kAnsvWin + 1]
-  int32_t* s_last = reinterpret_cast<int32_t*>(smem_raw + C::kKeyBytes);       // [NV][kAnsvRow]
-  int32_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
-  int32_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
-  int32_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
-  uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_rp + kTreeTile);            // [NV][MW]
-  uint8_t* s_e = reinterpret_cast<uint8_t*>(s_mask + NV * C::MW);              // [kAnsvWin]
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw + C::kKeyBytes);     // [NV][MW]
+  uint8_t* s_last = reinterpret_cast<uint8_t*>(s_mask + NV * C::MW);           // [NV][kAnsvRow]
+  uint8_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
+  uint8_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
+  uint8_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
+  uint8_t* s_e = s_rp + kTreeTile;                                             // [kAnsvWin]
   uint8_t* s_cmin = s_e + kAnsvWin;                                            // [kAnsvChunks]
 
   uint32_t first;
@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(kTreeThreads)
   // phase A: per chunk, E, the nearest smaller inside the chunk, and the
   // chunk's summaries (last / first position with E below each value)
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  static_assert(C::kKeyBytes % 4 == 0, "the masks follow the keys");
   // two chunks at a time per warp, so that their ballot chains interleave
   static_assert(kAnsvChunks % (2 * NW) == 0, "whole pairs of chunks per warp");
   for (int ch0 = int(warp); ch0 < kAnsvChunks; ch0 += 2 * NW) {
@@ -513,20 +514,19 @@ __global__ void __launch_bounds__(kTreeThreads)
       const uint32_t from0 = __shfl_sync(0xffffffffu, lt0[j], e[j] & 31);
       const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1[j], e[j] & 31) : 0u;
       const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
-      const int cbase = wlo + ch * 32;
       if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
         const int tg = (ch - kAnsvHalo) * 32 + int(lane);
         const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
-        s_lp[tg] = lm ? cbase + 31 - __clz(lm) : kAnsvNone;
-        s_rp[tg] = rm ? cbase + __ffs(rm) - 1 : kAnsvNoneR;
+        s_lp[tg] = lm ? uint8_t(31 - __clz(lm)) : uint8_t(0xff);
+        s_rp[tg] = rm ? uint8_t(__ffs(rm) - 1) : uint8_t(0xff);
       }
-      s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? cbase + 31 - __clz(lt0[j]) : kAnsvNone;
-      s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? cbase + __ffs(lt0[j]) - 1 : kAnsvNoneR;
+      s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(31 - __clz(lt0[j])) : uint8_t(0xff);
+      s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(__ffs(lt0[j]) - 1) : uint8_t(0xff);
       if (NV > 32) {
         s_last[(int(lane) + 32) * kAnsvRow + ch] =
-            lt1[j] ? cbase + 31 - __clz(lt1[j]) : kAnsvNone;
+            lt1[j] ? uint8_t(31 - __clz(lt1[j])) : uint8_t(0xff);
         s_first[(int(lane) + 32) * kAnsvRow + ch] =
-            lt1[j] ? cbase + __ffs(lt1[j]) - 1 : kAnsvNoneR;
+            lt1[j] ? uint8_t(__ffs(lt1[j]) - 1) : uint8_t(0xff);
       }
     }
   }
@@ -557,24 +557,27 @@ __global__ void __launch_bounds__(kTreeThreads)
     const int e = s_e[g - wlo];
     // not inside its own chunk: the nearest chunk on that side whose minimum
     // is below e holds the answer in its summary
-    int L = s_lp[tg];
+    const int cb = wlo + ch * 32;  // first gap of this chunk
+    int L = s_lp[tg] != 0xff ? cb + s_lp[tg] : kAnsvNone;
     if (L == kAnsvNone) {
       for (int wd = (ch - 1) >> 5; wd >= 0; --wd) {
         uint32_t bits = s_mask[e * C::MW + wd];
         if (wd == (ch - 1) >> 5) bits &= 0xffffffffu >> (31 - ((ch - 1) & 31));
         if (bits) {
-          L = s_last[e * kAnsvRow + wd * 32 + 31 - __clz(bits)];
+          const int c2 = wd * 32 + 31 - __clz(bits);
+          L = wlo + c2 * 32 + s_last[e * kAnsvRow + c2];
           break;
         }
       }
     }
-    int R = s_rp[tg];
+    int R = s_rp[tg] != 0xff ? cb + s_rp[tg] : kAnsvNoneR;
     if (R == kAnsvNoneR) {
       for (int wd = (ch + 1) >> 5; wd < C::MW; ++wd) {
         uint32_t bits = s_mask[e * C::MW + wd];
         if (wd == (ch + 1) >> 5) bits &= 0xffffffffu << ((ch + 1) & 31);
         if (bits) {
-          R = s_first[e * kAnsvRow + wd * 32 + __ffs(bits) - 1];
+          const int c2 = wd * 32 + __ffs(bits) - 1;
+          R = wlo + c2 * 32 + s_first[e * kAnsvRow + c2];
           break;
         }
       }
@@ -962,7 +965,7 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   uint32_t* far_n = sc.tile_ctr + kCtrTree;
-  const int far_blocks = std::max(1, sc.num_sms * 2);
+  const int far_blocks = std::max(1, sc.num_sms * 8);
   if (edges) {
     k_radix_tree<K, true><<<tiles, kTreeThreads, smem, s>>>(
         codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
