@@ -490,7 +490,7 @@ const char* rw_tree_pipeline_kernel_names(const rw_tree_im_storage* im) {
     names = "morton_histogram,sort_init";
     for (int p = 0; p < (im ? im->passes : 0); ++p) names += ",sort_pass" + std::to_string(p);
   }
-  names += ",unique,radix_tree_edges,edge_scan,octree_rows,octree_links";
+  names += ",unique,radix_tree_edges,edge_scan,octree,octree_far_links";
   return names.c_str();
 }
 

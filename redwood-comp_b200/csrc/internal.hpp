@@ -50,7 +50,7 @@ struct rw_tree_im_storage {
 
 namespace rwt {
 
-enum : int { kCtrUnique = 0, kCtrScan = 1, kCtrTree = 2, kCtrSortBase = 4,
+enum : int { kCtrUnique = 0, kCtrScan = 1, kCtrTree = 2, kCtrLinks = 3, kCtrSortBase = 4,
              kCtrSortClassStride = 8, kMaxSortClasses = 4, kCounters = 64 };
 
 // Tile sizes of the kernels (points or nodes per tile).
@@ -113,7 +113,9 @@ struct Scratch {
   uint32_t* scan_desc = nullptr;
   uint32_t* tile_ctr = nullptr;
   DevStatus* status = nullptr;
-  uint32_t* tree_far = nullptr;  // [tree_far_cap][2]: segment-global gap, segment
+  // [tree_far_cap][2]: radix-tree gaps left to the far search (gap, segment),
+  // then the octree's far links (node, segment)
+  uint32_t* tree_far = nullptr;
   uint32_t tree_far_cap = 0;
 };
 

@@ -792,45 +792,124 @@ __device__ __forceinline__ OctSeg oct_segment(const SegTable& seg, const OctOut&
   return r;
 }
 
-// Rows [off[i], off[i] + cnt[i]) belong to radix-tree node i (i >= 1).  Row
-// off+k sits at level L - k (L = prefix_n[i] / 3); for k > 0 its one chain
-// child is row off+k-1 (func_octree.hpp:56-78).  Node 0 owns no row; its
-// thread writes the root initialisation when there is no octree node at all
-// (07_octree.cu:188-198) and clears the spare row m that a top link may name.
+// Nearest ancestor of node c that owns rows: parents are followed while the
+// count is zero, at most 31 steps as in the reference (func_octree.hpp:80-92).
+// Returns -1 when a parent index is outside [0, n).
+__device__ __forceinline__ int link_parent(const int32_t* __restrict__ parents,
+                                           const int32_t* __restrict__ ec, int c, int n) {
+  int rp = parents[c];
+  if (uint32_t(rp) >= uint32_t(n)) return -1;
+  int counter = 0;
+  while (ec[rp] == 0) {
+    rp = parents[rp];
+    if (uint32_t(rp) >= uint32_t(n)) return -1;
+    if (++counter > 30) break;
+  }
+  return rp;
+}
+
+// The link of node c (count cnt > 0) into the global rows: child slot of the
+// chain's top row (level prefix_n[c] / 3 - cnt + 1) in row offset[rp]
+// (func_octree.hpp:94-102).  The reference overwrites in ascending node
+// order; the value off[c] + cnt - 1 grows with c, so the maximum is the last
+// write.
+template <typename K>
+__device__ __forceinline__ void link_global(const K* __restrict__ codes,
+                                            const uint8_t* __restrict__ prefix_n,
+                                            const int32_t* __restrict__ off, int c, int cnt,
+                                            int rp, const OctSeg& os, const OctOut& o) {
+  constexpr int B = KeyTraits<K>::kCodeBits;
+  const int oct_parent = off[rp];
+  const int top = prefix_n[c] / 3 - cnt + 1;
+  const int slot = int((codes[c] >> (B - 3 * top)) & K(7));
+  if (uint32_t(oct_parent) < os.cap) {
+    const size_t r = size_t(os.row0) + uint32_t(oct_parent);
+    atomicMax(o.children + 8 * r + slot, off[c] + cnt - 1);
+    atomicOr(o.node_mask + r, 1 << slot);
+  }
+}
+
+// Stage 7 in one pass over a tile of radix-tree nodes (func_octree.hpp:28-112).
+//
+// Rows [off[i], off[i] + cnt[i]) belong to node i (i >= 1); the offsets are
+// an exclusive scan of non-negative counts, so a tile of nodes owns one
+// contiguous run of rows, and the owner of row p is the last node whose
+// first row is <= p.  Row off+k sits at level L - k (L = prefix_n[i] / 3);
+// for k > 0 its one child is the chain row off+k-1 (func_octree.hpp:56-78).
+// A row with k = 0 gets its children only from links: the chain's top row
+// p = off[c] + cnt[c] - 1 of node c is named in row off[rp] of c's nearest
+// ancestor rp that owns rows (func_octree.hpp:80-111).  When rp lies in the
+// tile and owns rows, that row is a k = 0 row of the tile: the link is
+// merged in shared memory and every row is written once, complete.  Other
+// links go to the far list (node, segment), applied after this kernel with
+// global atomics; a list that overflows makes the far kernel apply every
+// link again (the atomics are idempotent).
+//
+// Threads take the tile's rows in turn (row r by thread r mod threads), so
+// that every lane has a row; the owner comes from a binary search over the
+// tile's first rows.
+//
+// Node 0 owns no row; tile 0 writes the root initialisation when there is
+// no octree row at all (07_octree.cu:188-198) and clears the spare row m
+// that a link may name.
 template <typename K>
 __global__ void __launch_bounds__(kOctThreads)
-    k_octree_rows(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
-                  const int32_t* __restrict__ ec_all, const int32_t* __restrict__ off_all,
-                  SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
-                  const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
-                  float min_coord, float range, OctOut o) {
+    k_octree(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
+             const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
+             const int32_t* __restrict__ off_all, SegTable seg, TileMap map,
+             const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ n_octree,
+             int32_t* __restrict__ seg_err, float min_coord, float range, OctOut o,
+             uint32_t* __restrict__ far, uint32_t far_cap, uint32_t* __restrict__ far_n) {
   constexpr int B = KeyTraits<K>::kCodeBits;
+  constexpr int kTile = int(kOctTile);
+  constexpr int kRowCap = 2 * kTile;  // rows whose owner is kept
+  static_assert(kTile < 0xfff && (kTile & (kTile - 1)) == 0, "12-bit parents, 2^k tile");
+  // k = 0 row of each node: child slot values relative to the tile's first
+  // row, plus one (0: no child), and the slots taken (one byte per node)
+  __shared__ uint4 s_child[kTile];  // 8 x u16
+  __shared__ uint32_t s_cmask[kTile / 4];
+  __shared__ int32_t s_off[kTile + 1];  // first row of each node; [kTile]: end of the tile's rows
+  __shared__ K s_code[kTile];
+  // per node: (count class << 12) | tile-relative parent (0xfff: outside);
+  // class 0: count 0, 1: count > 0, 2: count < 0
+  __shared__ uint16_t s_node[kTile];
+  __shared__ uint8_t s_level[kTile];  // prefix_n / 3
+  __shared__ uint16_t s_owner[kRowCap];
+
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
   const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c,
                                 blockIdx.x == first && threadIdx.x == 0);
   if (!os.ok) return;
+  const int n = os.n;
+  const int tile0 = int(blockIdx.x - first) * kTile;
+  if (tile0 >= n) return;
   const uint32_t sb = seg_begin(seg, c);
   const K* codes = codes_all + sb;
   const uint8_t* prefix_n = prefix_all + sb;
+  const int32_t* parents = parents_all + sb;
   const int32_t* ec = ec_all + sb;
   const int32_t* off = off_all + sb;
-  const int n = os.n;
   const uint32_t m = os.m;
-  const int root_level = prefix_n[0] / 3;
-  // a warp takes 32 consecutive nodes; their rows are one contiguous run
-  // (the offsets are an exclusive scan), written 32 rows at a time: the row
-  // of lane j belongs to the last lane whose first row is <= it (a lane with
-  // no rows shares its first row with the next lane, which is later)
-  const uint32_t lane = lane_id();
-  const int wnodes = (kOctThreads / 32) * kOctNpt;  // warp-groups per tile x 32
-  const int tile0 = int(blockIdx.x - first) * kOctTile;
-  for (int q = int(threadIdx.x >> 5); q < wnodes; q += kOctThreads / 32) {
-    const int i0 = tile0 + q * 32;
-    if (i0 >= n) break;
-    const int i = i0 + int(lane);
-    const bool valid = i < n;
-    if (i == 0) {
+  const int tile_end = min(tile0 + kTile, n);
+  const int tid = int(threadIdx.x);
+
+  for (int t = tid; t < kTile; t += kOctThreads) {
+    const int i = tile0 + t;
+    const bool valid = i < tile_end;
+    const int e = valid ? ec[i] : 0;
+    const int pa = valid ? parents[i] : -1;
+    const int pr = pa >= tile0 && pa < tile_end ? pa - tile0 : 0xfff;
+    s_node[t] = uint16_t((e == 0 ? 0 : e > 0 ? 1 : 2) << 12 | pr);
+    s_off[t] = valid ? off[i] : 0x7fffffff;
+    s_code[t] = valid ? codes[i] : K(0);
+    s_level[t] = valid ? uint8_t(prefix_n[i] / 3) : uint8_t(0);
+    s_child[t] = make_uint4(0, 0, 0, 0);
+  }
+  for (int t = tid; t < kTile / 4; t += kOctThreads) s_cmask[t] = 0;
+  if (tid == 0) {
+    s_off[kTile] = tile_end < n ? off[tile_end] : int(m);
+    if (tile0 == 0) {
       const size_t rm = size_t(os.row0) + m;
       int4* row = reinterpret_cast<int4*>(o.children + 8 * rm);
       row[0] = make_int4(0, 0, 0, 0);
@@ -838,98 +917,164 @@ __global__ void __launch_bounds__(kOctThreads)
       o.node_mask[rm] = 0;
       o.leaf_mask[rm] = 0;
       if (m == 0) {
+        const int root_level = prefix_n[0] / 3;
         const K pre = codes[0] >> (B - 3 * root_level);
         o.corner[os.row0] = decode<K>(K(pre << (B - 3 * root_level)), min_coord, range);
         o.cell_size[os.row0] = range;
       }
     }
-    const int cnt = (valid && i > 0) ? max(ec[i], 0) : 0;
-    const int off_l = valid ? off[i] : 0x7fffffff;
-    const K code = valid ? codes[i] : K(0);
-    const int li = valid ? prefix_n[i] / 3 : 0;
-    const int total = warp_sum(cnt);
-    if (total == 0) continue;
-    const int r0 = __shfl_sync(0xffffffffu, off_l, 0);
-    for (int t = 0; t < total; t += 32) {
-      const int p = r0 + t + int(lane);
-      int owner = 0;
+  }
+  __syncthreads();
+  if (tile_end < tile0 + kTile && tid == 0) s_off[tile_end - tile0] = s_off[kTile];
+  __syncthreads();
+
+  const int rbase = s_off[0];
+  const int rend = min(s_off[kTile], int(m));  // rows [rbase, rend)
+  const int root_level = prefix_n[0] / 3;
+  auto owner_of = [&](int p) -> int {  // last node whose first row is <= p
+    int t = 0;
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int o_off = __shfl_sync(0xffffffffu, off_l, owner + step);
-        if (owner + step < 32 && o_off <= p) owner += step;
+    for (int step = kTile / 2; step >= 1; step >>= 1)
+      if (s_off[t + step] <= p) t += step;
+    return t;
+  };
+
+  // links, from the chain top rows; the walk of link_parent over the tile's
+  // counts and parents.  A walk that leaves the tile or ends on a node
+  // without rows, and a value that does not fit 16 bits, go to the far list
+  // (which repeats the whole walk in global memory and merges with
+  // atomics).  Several links may name one slot (the reference keeps the
+  // last, the largest value): the 16-bit maximum is taken with
+  // compare-and-swap on the slot's word.
+  for (int r = tid; rbase + r < rend; r += kOctThreads) {
+    const int p = rbase + r;
+    const int t = owner_of(p);
+    if (r < kRowCap) s_owner[r] = uint16_t(t);
+    if (p != s_off[t + 1] - 1) continue;  // not the top row of its chain
+    const uint32_t w0 = s_node[t];
+    int rp = int(w0 & 0xfffu), counter = 0;
+    bool local = rp != 0xfff;
+    uint32_t w = 0;
+    while (local) {
+      w = s_node[rp];
+      if (w >> 12) break;
+      if ((w & 0xfffu) == 0xfffu || ++counter > 30) local = false;
+      rp = int(w & 0xfffu);
+    }
+    if (local && (w >> 12) == 1 && r < 0xffff) {
+      const int level = int(s_level[t]) - (p - s_off[t]);  // the top row's level
+      const int slot = int((s_code[t] >> (B - 3 * level)) & K(7));
+      uint32_t* wp = reinterpret_cast<uint32_t*>(&s_child[rp]) + (slot >> 1);
+      const int sh = 16 * (slot & 1);
+      const uint32_t rel = uint32_t(r) + 1u;  // the link value is p itself
+      uint32_t cur = *reinterpret_cast<volatile uint32_t*>(wp);
+      bool done = false;
+      for (int tries = 0; tries < 64 && !done; ++tries) {  // each failure is another's success
+        if (((cur >> sh) & 0xffffu) >= rel) {
+          done = true;
+        } else {
+          const uint32_t nv = (cur & ~(0xffffu << sh)) | (rel << sh);
+          const uint32_t prev = atomicCAS(wp, cur, nv);
+          done = prev == cur;
+          cur = prev;
+        }
       }
-      const int o_off = __shfl_sync(0xffffffffu, off_l, owner);
-      const int o_li = __shfl_sync(0xffffffffu, li, owner);
-      const K o_code = __shfl_sync(0xffffffffu, code, owner);
-      if (t + int(lane) >= total || uint32_t(p) >= m) continue;
-      const size_t rp = size_t(os.row0) + uint32_t(p);
-      const int k = p - o_off;
-      const int level = o_li - k;
-      const K pre = o_code >> (B - 3 * level);
-      o.corner[rp] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
-      // range / 2^s, s = level - root_level in [0, 21]: the product with the
-      // exact reciprocal 2^-s is the same correctly rounded value
-      o.cell_size[rp] = __fmul_rn(range, __uint_as_float(uint32_t(127 - (level - root_level)) << 23));
-      int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      int32_t mask = 0;
-      if (k > 0) {
-        const int slot = int((o_code >> (B - 3 * (level + 1))) & K(7));
-        child[slot] = p - 1;
-        mask = 1 << slot;
+      if (done) {
+        atomicOr(&s_cmask[rp >> 2], 1u << (slot + 8 * (rp & 3)));
+        continue;
       }
-      int4* row = reinterpret_cast<int4*>(o.children + 8 * rp);
+    }
+    const uint32_t at = atomicAdd(far_n, 1u);
+    if (at < far_cap) {
+      far[2 * at] = uint32_t(tile0 + t);
+      far[2 * at + 1] = c;
+    }
+  }
+  __syncthreads();
+
+  // rows
+  for (int r = tid; rbase + r < rend; r += kOctThreads) {
+    const int p = rbase + r;
+    const int t = r < kRowCap ? int(s_owner[r]) : owner_of(p);
+    const size_t rp = size_t(os.row0) + uint32_t(p);
+    const int k = p - s_off[t];
+    const int level = int(s_level[t]) - k;
+    const K code = s_code[t];
+    const K pre = code >> (B - 3 * level);
+    o.corner[rp] = decode<K>(K(pre << (B - 3 * level)), min_coord, range);
+    // range / 2^s, s = level - root_level in [0, 21]: the product with the
+    // exact reciprocal 2^-s is the same correctly rounded value
+    o.cell_size[rp] =
+        __fmul_rn(range, __uint_as_float(uint32_t(127 - (level - root_level)) << 23));
+    int4* row = reinterpret_cast<int4*>(o.children + 8 * rp);
+    if (k == 0) {
+      const uint4 a = s_child[t];
+      const uint32_t wv[4] = {a.x, a.y, a.z, a.w};
+      int32_t child[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t v = (wv[q >> 1] >> (16 * (q & 1))) & 0xffffu;
+        child[q] = v ? int32_t(v) - 1 + rbase : 0;
+      }
       row[0] = make_int4(child[0], child[1], child[2], child[3]);
       row[1] = make_int4(child[4], child[5], child[6], child[7]);
-      o.node_mask[rp] = mask;
-      o.leaf_mask[rp] = 0;
+      o.node_mask[rp] = int32_t((s_cmask[t >> 2] >> (8 * (t & 3))) & 0xffu);
+    } else {
+      int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      const int slot = int((code >> (B - 3 * (level + 1))) & K(7));
+      child[slot] = p - 1;
+      row[0] = make_int4(child[0], child[1], child[2], child[3]);
+      row[1] = make_int4(child[4], child[5], child[6], child[7]);
+      o.node_mask[rp] = 1 << slot;
     }
+    o.leaf_mask[rp] = 0;
   }
 }
 
-// Link of each chain's top row to the row of the nearest ancestor that owns
-// rows (func_octree.hpp:80-111; the walk gives up after 31 steps as there).
+// Links that k_octree left to the far list, with global atomics; when the
+// list overflowed, every node's link again (blocks stride over all tiles).
 template <typename K>
-__global__ void __launch_bounds__(kOctThreads)
-    k_octree_links(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
-                   const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
-                   const int32_t* __restrict__ off_all, SegTable seg, TileMap map,
-                   const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ n_octree,
-                   int32_t* __restrict__ seg_err, OctOut o) {
-  constexpr int B = KeyTraits<K>::kCodeBits;
-  uint32_t first;
-  const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
-  const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
-  if (!os.ok) return;
-  const uint32_t sb = seg_begin(seg, c);
-  const K* codes = codes_all + sb;
-  const uint8_t* prefix_n = prefix_all + sb;
-  const int32_t* parents = parents_all + sb;
-  const int32_t* ec = ec_all + sb;
-  const int32_t* off = off_all + sb;
-  const int n = os.n;
-  const int base = int(blockIdx.x - first) * kOctTile;
-  for (int q = 0; q < kOctNpt; ++q) {
-    const int i = base + q * kOctThreads + int(threadIdx.x);
-    if (i >= n) break;
-    if (i == 0) continue;
-    const int cnt = ec[i];
-    if (cnt <= 0) continue;
-    int rp = parents[i];
-    if (uint32_t(rp) >= uint32_t(n)) continue;
-    int counter = 0;
-    while (ec[rp] == 0) {
-      rp = parents[rp];
-      if (uint32_t(rp) >= uint32_t(n)) break;
-      if (++counter > 30) break;
+__global__ void __launch_bounds__(256)
+    k_octree_far_links(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
+                       const int32_t* __restrict__ parents_all,
+                       const int32_t* __restrict__ ec_all, const int32_t* __restrict__ off_all,
+                       SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
+                       const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
+                       OctOut o, const uint32_t* __restrict__ far, uint32_t far_cap,
+                       const uint32_t* __restrict__ far_n) {
+  const uint32_t count = *far_n;
+  if (count <= far_cap) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
+         w += gridDim.x * blockDim.x) {
+      const int i = int(far[2 * w]);
+      const uint32_t c = far[2 * w + 1];
+      const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
+      if (!os.ok) continue;
+      const uint32_t sb = seg_begin(seg, c);
+      const int rp = link_parent(parents_all + sb, ec_all + sb, i, os.n);
+      if (rp < 0) continue;
+      link_global<K>(codes_all + sb, prefix_all + sb, off_all + sb, i, ec_all[sb + i], rp,
+                     os, o);
     }
-    if (uint32_t(rp) >= uint32_t(n)) continue;
-    const int oct_parent = off[rp];
-    const int top = prefix_n[i] / 3 - cnt + 1;
-    const int slot = int((codes[i] >> (B - 3 * top)) & K(7));
-    if (uint32_t(oct_parent) < os.cap) {
-      const size_t r = size_t(os.row0) + uint32_t(oct_parent);
-      atomicMax(o.children + 8 * r + slot, off[i] + cnt - 1);
-      atomicOr(o.node_mask + r, 1 << slot);
+    return;
+  }
+  for (uint32_t tile = blockIdx.x; tile < map.n_tiles; tile += gridDim.x) {
+    uint32_t first;
+    const uint32_t c = tile_segment(seg, map, tile, &first);
+    const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
+    if (!os.ok) continue;
+    const uint32_t sb = seg_begin(seg, c);
+    const int32_t* ec = ec_all + sb;
+    const int base = int(tile - first) * int(kOctTile);
+    for (int q = int(threadIdx.x); q < int(kOctTile); q += int(blockDim.x)) {
+      const int i = base + q;
+      if (i >= os.n) break;
+      if (i == 0) continue;
+      const int cnt = ec[i];
+      if (cnt <= 0) continue;
+      const int rp = link_parent(parents_all + sb, ec, i, os.n);
+      if (rp < 0) continue;
+      link_global<K>(codes_all + sb, prefix_all + sb, off_all + sb, i, cnt, rp, os, o);
     }
   }
 }
@@ -987,23 +1132,25 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
 template <typename K>
 cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
                      cudaEvent_t* marks) {
-  (void)sc;
   OctOut o{b.children, b.corner, b.cell_size, b.node_mask, b.leaf_mask, pl.oct_off,
            pl.oct_capacity};
   const K* codes = static_cast<const K*>(b.keys);
   const uint32_t tiles = pl.node_map.n_tiles;
+  uint32_t* far_n = sc.tile_ctr + kCtrLinks;
+  cudaError_t e = cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
   if (tiles)
-    k_octree_rows<K><<<tiles, kOctThreads, 0, s>>>(
-        codes, b.prefix_n, b.edge_count, b.edge_offset, pl.seg, pl.node_map, pl.n_unique,
-        pl.n_octree, pl.seg_err, b.min_coord, b.range, o);
-  cudaError_t e = cudaGetLastError();
+    k_octree<K><<<tiles, kOctThreads, 0, s>>>(
+        codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, pl.seg, pl.node_map,
+        pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o, sc.tree_far,
+        sc.tree_far_cap, far_n);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
   if (tiles)
-    k_octree_links<K><<<tiles, kOctThreads, 0, s>>>(codes, b.prefix_n, b.parents,
-                                                    b.edge_count, b.edge_offset, pl.seg,
-                                                    pl.node_map, pl.n_unique, pl.n_octree,
-                                                    pl.seg_err, o);
+    k_octree_far_links<K><<<std::max(1, sc.num_sms * 4), 256, 0, s>>>(
+        codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, pl.seg, pl.node_map,
+        pl.n_unique, pl.n_octree, pl.seg_err, o, sc.tree_far, sc.tree_far_cap, far_n);
   e = cudaGetLastError();
   if (e == cudaSuccess && marks) cudaEventRecord(marks[1], s);
   return e;
