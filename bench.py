@@ -614,32 +614,41 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     single_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
-    # two slots on two streams: submit(k) then collect(k-1), so one cloud's
-    # copies out overlap the next cloud's copies in and its pipeline
-    app2 = rw.AppData(a.n, a.key_bits, points=pts)
-    im2 = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
-    if a.sort_variant >= 0:
-        im2.set_sort_variant(a.sort_variant)
-    outs2 = {k: torch.empty_like(v).pin_memory().numpy() for k, v in outs.items()}
-    slots = [(app, im, torch.cuda.Stream(), outs_np), (app2, im2, torch.cuda.Stream(), outs2)]
+    # three slots on three streams: submit(k) then collect(k-2).  A slot's
+    # stream runs copy in, pipeline, copy out in order; with three slots the
+    # copy in of cloud k does not wait behind the copy out of the cloud before
+    # it on the same stream while another cloud's copy out holds the
+    # device-to-host direction
+    n_slots = 3
+    slots = [(app, im, torch.cuda.Stream(), outs_np)]
+    for _ in range(n_slots - 1):
+        ax = rw.AppData(a.n, a.key_bits, points=pts)
+        ix = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
+        if a.sort_variant >= 0:
+            ix.set_sort_variant(a.sort_variant)
+        slots.append((ax, ix, torch.cuda.Stream(),
+                      {k: torch.empty_like(v).pin_memory().numpy() for k, v in outs.items()}))
 
     def streamed(k_steps):
-        rw.host_submit(slots[0][0], slots[0][1], h_np, slots[0][2])
-        for k in range(1, k_steps):
-            cur, prev = slots[k % 2], slots[(k - 1) % 2]
-            rw.host_submit(cur[0], cur[1], h_np, cur[2])
-            rw.host_collect(prev[0], prev[1], prev[3], prev[2])
-        last = slots[(k_steps - 1) % 2]
-        rw.host_collect(last[0], last[1], last[3], last[2])
+        lag = n_slots - 1
+        for k in range(k_steps + lag):
+            if k < k_steps:
+                cur = slots[k % n_slots]
+                rw.host_submit(cur[0], cur[1], h_np, cur[2])
+            if k >= lag:
+                prev = slots[(k - lag) % n_slots]
+                rw.host_collect(prev[0], prev[1], prev[3], prev[2])
 
     streamed(4)
     torch.cuda.synchronize()
     barrier()
-    s0, s1 = slots[0][2], slots[1][2]
+    s0 = slots[0][2]
     e0.record(s0)
-    s1.wait_event(e0)
+    for sl in slots[1:]:
+        sl[2].wait_event(e0)
     streamed(e2e_steps)
-    s0.wait_stream(s1)
+    for sl in slots[1:]:
+        s0.wait_stream(sl[2])
     e1.record(s0)
     torch.cuda.synchronize()
     barrier()
@@ -650,10 +659,10 @@ def main():
            "h2d_bytes_per_step": 16 * a.n, "d2h_bytes_per_step": d2h,
            "ms_per_step": round(e2e_ms, 4),
            "single_slot_ms_per_step": round(single_ms, 4),
-           "path": "rw_tree_host_submit / rw_tree_host_collect on two AppData/scratch pairs "
-                   "and two streams: pinned host points -> H2D -> 7 stages -> counts + "
+           "path": "rw_tree_host_submit / rw_tree_host_collect on three AppData/scratch "
+                   "pairs and three streams: pinned host points -> H2D -> 7 stages -> counts + "
                    "octree rows (children, corner, cell_size, masks) D2H, every step"}
-    del app2, im2
+    del slots[1:]
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -1148,7 +1148,7 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
   if (tiles)
-    k_octree_far_links<K><<<std::max(1, sc.num_sms * 4), 256, 0, s>>>(
+    k_octree_far_links<K><<<std::max(1, sc.num_sms * 8), 256, 0, s>>>(
         codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, pl.seg, pl.node_map,
         pl.n_unique, pl.n_octree, pl.seg_err, o, sc.tree_far, sc.tree_far_cap, far_n);
   e = cudaGetLastError();
