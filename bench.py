@@ -154,21 +154,22 @@ def kernel_bytes(name, n, u, m, K):
         # codes read; prefix_n, 2 leaf flags, left_child, parent, edge count written
         return K * u + 15 * b
     if name == "edge_scan":
-        return 8 * b
+        # counts read (per-tile sums; the offsets are written by the octree kernel)
+        return 4 * b
     if name == "octree":
-        # codes, prefix_n, count, offset, parent read; corner 16 + cell 4 + children 32
-        # + masks 8 written (links merged in shared memory)
+        # codes, prefix_n, count, parent read, offset written; corner 16 + cell 4
+        # + children 32 + masks 8 written (links merged in shared memory)
         return (K + 13) * b + 60 * m
     return 0
 
 
 def pipeline_bytes(n, u, m, K, passes):
     """Whole-pipeline algorithmic bytes (per-stage formulas: S1 (16+K)n,
-    S2 K n (1+2P), S3 K(n+u), S4 K u + 11 b, S5 10 b, S6 8 b,
-    S7 (13+K) b + 60 m)."""
+    S2 K n (1+2P), S3 K(n+u), S4 K u + 11 b, S5 10 b, S6 4 b,
+    S7 (13+K) b + 60 m; stage 6's offsets are written inside stage 7)."""
     b = u - 1
     return ((16 + K) * n + K * n * (1 + 2 * passes) + K * (n + u) + K * u + 11 * b
-            + 10 * b + 8 * b + (13 + K) * b + 60 * m)
+            + 10 * b + 4 * b + (13 + K) * b + 60 * m)
 
 
 def traffic_table():

@@ -271,7 +271,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   const size_t ghist_b = align(size_t(n_clouds) * b->passes * radix * 4);
   const size_t sdesc_b = align(size_t(b->passes) * b->sort_rows * radix * 4);
   const size_t udesc_b = align((size_t(b->unique_tiles) + 1) * 4);
-  const size_t cdesc_b = align((size_t(b->scan_tiles) + 1) * 4);
+  const size_t cdesc_b = align((size_t(std::max(b->scan_tiles, b->node_tiles)) + 1) * 4);
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
   const size_t per_b = align(size_t(n_clouds) * 4);
@@ -412,8 +412,8 @@ int rw_tree_batch_enqueue(rw_tree_batch* b, const rw_tree_batch_buffers* u, rw_s
   }
   RWB_CUDA(rwt::launch_unique(x, sc, pl, s));
   RWB_CUDA(rwt::launch_radix_tree(x, sc, pl, true, s));
-  RWB_CUDA(rwt::launch_edge_scan(x, sc, pl, s));
-  RWB_CUDA(rwt::launch_octree(x, sc, pl, s));
+  RWB_CUDA(rwt::launch_edge_sums(x, sc, pl, s));
+  RWB_CUDA(rwt::launch_octree(x, sc, pl, s, nullptr, true));
   const size_t c = b->n_clouds;
   RWB_CUDA(cudaMemcpyAsync(b->h_results, b->d_n_unique, 4 * c, cudaMemcpyDeviceToHost, s));
   RWB_CUDA(cudaMemcpyAsync(b->h_results + c, b->d_n_octree, 4 * c, cudaMemcpyDeviceToHost, s));

@@ -210,7 +210,9 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
   const size_t ghist_b = align(size_t(im->passes) * radix * 4);
   const size_t sdesc_b = align(size_t(im->passes) * (im->sort_tiles + 1) * radix * 4);
   const size_t udesc_b = align((size_t(rwt::div_up(n_input, rwt::kUniqueTile)) + 1) * 4);
-  const size_t cdesc_b = align((size_t(rwt::div_up(n_input, rwt::kScanTile)) + 1) * 4);
+  // stage 6's tiles, or the octree's (smaller) ones in the fused pipeline
+  const size_t cdesc_b = align((size_t(rwt::div_up(n_input, rwt::kOctTile)) + 1) * 4);
+  static_assert(rwt::kOctTile <= rwt::kScanTile, "scan descriptors sized by the octree tiles");
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
   im->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b;
@@ -465,9 +467,9 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
   RW_CUDA(mark());
   RW_CUDA(rwt::launch_radix_tree(b, sc, pl, true, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_edge_scan(b, sc, pl, s));
+  RW_CUDA(rwt::launch_edge_sums(b, sc, pl, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_octree(b, sc, pl, s, ev ? ev + k : nullptr));
+  RW_CUDA(rwt::launch_octree(b, sc, pl, s, ev ? ev + k : nullptr, true));
   if (ev) k += 2;
   RW_CUDA(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(rwt::DevStatus),
                           cudaMemcpyDeviceToHost, s));

@@ -163,8 +163,12 @@ cudaError_t launch_radix_tree(const Bufs& b, const Scratch& sc, const Plan& pl, 
 cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
                               cudaStream_t s);
 cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
+// The first half of stage 6 on the octree's tiles: each tile's count sum,
+// scanned into sc.scan_desc, and the octree row counts.  launch_octree with
+// fused_offsets then makes and writes the offsets itself.
+cudaError_t launch_edge_sums(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
 cudaError_t launch_octree(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
-                          cudaEvent_t* marks = nullptr);
+                          cudaEvent_t* marks = nullptr, bool fused_offsets = false);
 
 // Text returned by rw_tree_last_error (this thread).
 void set_last_error(const std::string& msg);

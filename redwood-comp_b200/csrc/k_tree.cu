@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(1024)
     k_tile_scan(uint32_t* __restrict__ E, uint32_t tiles, SegTable seg, TileMap map,
                 uint32_t* __restrict__ seg_total) {
   __shared__ uint32_t s_warp[33];
-  constexpr int R = 8;
+  constexpr int R = 16;  // 16,384 tiles per round
   uint32_t carry = 0;
   for (uint32_t c0 = 0; c0 < tiles; c0 += 1024 * R) {
     const uint32_t f = c0 + threadIdx.x * R;
@@ -852,14 +852,20 @@ __device__ __forceinline__ void link_global(const K* __restrict__ codes,
 // Node 0 owns no row; tile 0 writes the root initialisation when there is
 // no octree row at all (07_octree.cu:188-198) and clears the spare row m
 // that a link may name.
-template <typename K>
+//
+// With OFFS the offsets are not read but made here (stage 6's write folded
+// into stage 7): tile_prefix holds the exclusive scan of every tile's count
+// sum (k_node_sums, k_tile_scan), the block scans its tile's counts on top
+// of it and writes them to off_all.
+template <typename K, bool OFFS>
 __global__ void __launch_bounds__(kOctThreads)
     k_octree(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
              const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
-             const int32_t* __restrict__ off_all, SegTable seg, TileMap map,
-             const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ n_octree,
-             int32_t* __restrict__ seg_err, float min_coord, float range, OctOut o,
-             uint32_t* __restrict__ far, uint32_t far_cap, uint32_t* __restrict__ far_n) {
+             int32_t* __restrict__ off_all, const uint32_t* __restrict__ tile_prefix,
+             SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
+             const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
+             float min_coord, float range, OctOut o, uint32_t* __restrict__ far,
+             uint32_t far_cap, uint32_t* __restrict__ far_n) {
   constexpr int B = KeyTraits<K>::kCodeBits;
   constexpr int kTile = int(kOctTile);
   constexpr int kRowCap = 2 * kTile;  // rows whose owner is kept
@@ -875,6 +881,9 @@ __global__ void __launch_bounds__(kOctThreads)
   __shared__ uint16_t s_node[kTile];
   __shared__ uint8_t s_level[kTile];  // prefix_n / 3
   __shared__ uint16_t s_owner[kRowCap];
+  __shared__ uint32_t s_wsum[4 * (kOctThreads / 32) + 1];
+  static_assert(kTile == 4 * kOctThreads && 4 * (kOctThreads / 32) == 32,
+                "four groups of 256 nodes, 32 warp sums");
 
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
@@ -889,26 +898,63 @@ __global__ void __launch_bounds__(kOctThreads)
   const uint8_t* prefix_n = prefix_all + sb;
   const int32_t* parents = parents_all + sb;
   const int32_t* ec = ec_all + sb;
-  const int32_t* off = off_all + sb;
+  int32_t* off = off_all + sb;
   const uint32_t m = os.m;
   const int tile_end = min(tile0 + kTile, n);
   const int tid = int(threadIdx.x);
 
-  for (int t = tid; t < kTile; t += kOctThreads) {
+  // thread tid: nodes tile0 + tid + 256 q, q < 4 (coalesced loads)
+  int ev[4], ov[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t = tid + q * kOctThreads;
     const int i = tile0 + t;
     const bool valid = i < tile_end;
-    const int e = valid ? ec[i] : 0;
+    ev[q] = valid ? ec[i] : 0;
     const int pa = valid ? parents[i] : -1;
     const int pr = pa >= tile0 && pa < tile_end ? pa - tile0 : 0xfff;
-    s_node[t] = uint16_t((e == 0 ? 0 : e > 0 ? 1 : 2) << 12 | pr);
-    s_off[t] = valid ? off[i] : 0x7fffffff;
+    s_node[t] = uint16_t((ev[q] == 0 ? 0 : ev[q] > 0 ? 1 : 2) << 12 | pr);
+    ov[q] = (!OFFS && valid) ? off[i] : 0;
     s_code[t] = valid ? codes[i] : K(0);
     s_level[t] = valid ? uint8_t(prefix_n[i] / 3) : uint8_t(0);
     s_child[t] = make_uint4(0, 0, 0, 0);
   }
+  uint32_t rows_end = 0;
+  if (OFFS) {
+    // exclusive scan of the counts in node order, as stage 6 computes it: a
+    // warp scan per group of 32 nodes, then one warp scans the 32 group sums
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t inc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      inc[q] = warp_inclusive_scan(uint32_t(ev[q]));
+      if (lane == 31) s_wsum[q * (kOctThreads / 32) + warp] = inc[q];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t v = s_wsum[lane];
+      const uint32_t wi = warp_inclusive_scan(v);
+      s_wsum[lane] = wi - v;
+      if (lane == 31) s_wsum[32] = wi;
+    }
+    __syncthreads();
+    const uint32_t base = tile_prefix[blockIdx.x] - tile_prefix[first];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ov[q] = int32_t(base + s_wsum[q * (kOctThreads / 32) + warp] + inc[q] - uint32_t(ev[q]));
+      const int i = tile0 + tid + q * kOctThreads;
+      if (i < tile_end) off[i] = ov[q];
+    }
+    rows_end = base + s_wsum[32];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t = tid + q * kOctThreads;
+    s_off[t] = tile0 + t < tile_end ? ov[q] : 0x7fffffff;
+  }
   for (int t = tid; t < kTile / 4; t += kOctThreads) s_cmask[t] = 0;
   if (tid == 0) {
-    s_off[kTile] = tile_end < n ? off[tile_end] : int(m);
+    s_off[kTile] = OFFS ? int(rows_end) : (tile_end < n ? off[tile_end] : int(m));
     if (tile0 == 0) {
       const size_t rm = size_t(os.row0) + m;
       int4* row = reinterpret_cast<int4*>(o.children + 8 * rm);
@@ -1031,6 +1077,44 @@ __global__ void __launch_bounds__(kOctThreads)
   }
 }
 
+// Sum of the edge counts of every tile of kOctTile nodes (the tiles of
+// k_octree), for k_tile_scan: stage 6's reduce on the octree's tiles.  A block
+// takes four tiles, 64 threads and 16 consecutive nodes per thread each.
+__global__ void __launch_bounds__(kOctThreads)
+    k_node_sums(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
+                const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E) {
+  constexpr int kPer = int(kOctTile) / 64;  // nodes per thread
+  static_assert(kOctThreads == 256 && kPer % 4 == 0, "four tiles of 64 threads");
+  __shared__ uint32_t s_warp[kOctThreads / 32];
+  const uint32_t g = threadIdx.x >> 6;  // tile of this thread's group
+  const uint32_t tile = 4 * blockIdx.x + g;
+  uint32_t local = 0;
+  if (tile < map.n_tiles) {
+    uint32_t first;
+    const uint32_t c = tile_segment(seg, map, tile, &first);
+    const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
+    const bool ok = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, c);
+    const int n = ok ? int(nu - 1) : 0;
+    const int i0 = int(tile - first) * int(kOctTile) + int(threadIdx.x & 63u) * kPer;
+    const int32_t* ec = ec_all + seg_begin(seg, c);
+    if (i0 + kPer <= n && (reinterpret_cast<uintptr_t>(ec + i0) & 15u) == 0) {
+#pragma unroll
+      for (int q = 0; q < kPer / 4; ++q) {
+        const int4 x = reinterpret_cast<const int4*>(ec + i0)[q];
+        local += uint32_t(x.x) + uint32_t(x.y) + uint32_t(x.z) + uint32_t(x.w);
+      }
+    } else {
+      for (int q = 0; q < kPer; ++q)
+        if (i0 + q < n) local += uint32_t(ec[i0 + q]);
+    }
+  }
+  local = warp_sum(local);
+  if (lane_id() == 0) s_warp[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x < 4 && 4 * blockIdx.x + threadIdx.x < map.n_tiles)
+    E[4 * blockIdx.x + threadIdx.x] = s_warp[2 * threadIdx.x] + s_warp[2 * threadIdx.x + 1];
+}
+
 // Links that k_octree left to the far list, with global atomics; when the
 // list overflowed, every node's link again (blocks stride over all tiles).
 template <typename K>
@@ -1131,7 +1215,7 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
 
 template <typename K>
 cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
-                     cudaEvent_t* marks) {
+                     cudaEvent_t* marks, bool fused_offsets) {
   OctOut o{b.children, b.corner, b.cell_size, b.node_mask, b.leaf_mask, pl.oct_off,
            pl.oct_capacity};
   const K* codes = static_cast<const K*>(b.keys);
@@ -1139,11 +1223,18 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   uint32_t* far_n = sc.tile_ctr + kCtrLinks;
   cudaError_t e = cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  if (tiles)
-    k_octree<K><<<tiles, kOctThreads, 0, s>>>(
-        codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, pl.seg, pl.node_map,
-        pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o, sc.tree_far,
-        sc.tree_far_cap, far_n);
+  if (tiles) {
+    if (fused_offsets)
+      k_octree<K, true><<<tiles, kOctThreads, 0, s>>>(
+          codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, sc.scan_desc, pl.seg,
+          pl.node_map, pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o,
+          sc.tree_far, sc.tree_far_cap, far_n);
+    else
+      k_octree<K, false><<<tiles, kOctThreads, 0, s>>>(
+          codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, nullptr, pl.seg,
+          pl.node_map, pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o,
+          sc.tree_far, sc.tree_far_cap, far_n);
+  }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
@@ -1204,10 +1295,19 @@ cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, c
   return cudaGetLastError();
 }
 
+cudaError_t launch_edge_sums(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
+  const uint32_t tiles = pl.node_map.n_tiles;
+  if (!tiles) return cudaSuccess;
+  k_node_sums<<<div_up(tiles, 4), kOctThreads, 0, s>>>(b.edge_count, pl.seg, pl.node_map,
+                                                      pl.n_unique, sc.scan_desc);
+  k_tile_scan<<<1, 1024, 0, s>>>(sc.scan_desc, tiles, pl.seg, pl.node_map, pl.n_octree);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_octree(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
-                          cudaEvent_t* marks) {
-  return b.key_bits == 32 ? octree_t<uint32_t>(b, sc, pl, s, marks)
-                          : octree_t<uint64_t>(b, sc, pl, s, marks);
+                          cudaEvent_t* marks, bool fused_offsets) {
+  return b.key_bits == 32 ? octree_t<uint32_t>(b, sc, pl, s, marks, fused_offsets)
+                          : octree_t<uint64_t>(b, sc, pl, s, marks, fused_offsets);
 }
 
 Plan single_plan(uint32_t n, uint32_t oct_capacity, DevStatus* status, uint32_t sort_tile) {
