@@ -116,6 +116,57 @@ __device__ __forceinline__ uint32_t tile_heads(const K* __restrict__ sorted, uin
   return count;
 }
 
+// The same head flags for a warp whose 32 * kUniqueKpt keys are all in the
+// segment and start on a 16-byte boundary: vector j of lane l holds keys
+// wbase + (32 j + l) V + [0, V) (V keys per 16 bytes); hm[j] bit e flags key e
+// of that vector.
+template <typename K>
+struct UniqueVec {
+  static constexpr int V = 16 / int(sizeof(K));
+  static constexpr int NVEC = int(kUniqueKpt) / V;
+};
+
+template <typename K>
+__device__ __forceinline__ bool unique_vec_ok(const K* sorted, uint32_t wbase, uint32_t n) {
+  return wbase + 32u * kUniqueKpt <= n &&
+         (reinterpret_cast<uintptr_t>(sorted + wbase) & 15u) == 0;
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t tile_heads_vec(const K* __restrict__ sorted, uint32_t sb,
+                                                   uint32_t wbase, K (&keys)[kUniqueKpt],
+                                                   uint32_t (&hm)[UniqueVec<K>::NVEC]) {
+  constexpr int V = UniqueVec<K>::V, NVEC = UniqueVec<K>::NVEC;
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int j = 0; j < NVEC; ++j) {
+    const uint4 x = *reinterpret_cast<const uint4*>(sorted + wbase + (32u * j + lane) * V);
+    const K* xk = reinterpret_cast<const K*>(&x);
+#pragma unroll
+    for (int e = 0; e < V; ++e) keys[j * V + e] = xk[e];
+  }
+  const K before = (lane == 0 && wbase > sb) ? sorted[wbase - 1] : K(0);
+  K carry = K(0);
+  uint32_t count = 0;
+#pragma unroll
+  for (int j = 0; j < NVEC; ++j) {
+    const K last = keys[j * V + V - 1];
+    K up = __shfl_up_sync(0xffffffffu, last, 1);
+    if (lane == 0) up = j == 0 ? (wbase > sb ? before : K(~keys[0])) : carry;
+    carry = __shfl_sync(0xffffffffu, last, 31);
+    uint32_t m = 0;
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const K prev = e == 0 ? up : keys[j * V + e - 1];
+      const uint32_t idx = wbase + (32u * j + lane) * V + e;
+      m |= uint32_t(idx == sb || keys[j * V + e] != prev) << e;
+    }
+    hm[j] = m;
+    count += __popc(m);
+  }
+  return count;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
     k_unique_count(const K* __restrict__ sorted, SegTable seg, TileMap map,
@@ -129,8 +180,14 @@ __global__ void __launch_bounds__(kUniqueThreads)
   const uint32_t n = sb + seg_size(seg, c);
   const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * kUniqueKpt;
   K keys[kUniqueKpt];
-  uint32_t heads[kUniqueKpt];
-  const uint32_t count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  uint32_t count;
+  if (unique_vec_ok(sorted, wbase, n)) {
+    uint32_t hm[UniqueVec<K>::NVEC];
+    count = warp_sum(tile_heads_vec(sorted, sb, wbase, keys, hm));
+  } else {
+    uint32_t heads[kUniqueKpt];
+    count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  }
   if (lane == 0) s_warp[warp] = count;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -153,8 +210,18 @@ __global__ void __launch_bounds__(kUniqueThreads)
   const uint32_t n = sb + seg_size(seg, c);
   const uint32_t wbase = sb + (tile - first) * kUniqueTile + warp * 32u * kUniqueKpt;
   K keys[kUniqueKpt];
-  uint32_t heads[kUniqueKpt];
-  const uint32_t count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  constexpr int V = UniqueVec<K>::V, NVEC = UniqueVec<K>::NVEC;
+  const bool vec = unique_vec_ok(sorted, wbase, n);
+  uint32_t heads[kUniqueKpt];  // scalar path: ballots; vector path: hm[j] in heads[j]
+  uint32_t count;
+  if (vec) {
+    uint32_t hm[NVEC];
+    count = warp_sum(tile_heads_vec(sorted, sb, wbase, keys, hm));
+#pragma unroll
+    for (int j = 0; j < NVEC; ++j) heads[j] = hm[j];
+  } else {
+    count = tile_heads(sorted, sb, n, wbase, keys, heads);
+  }
   if (lane == 0) s_warp[warp] = count;
   __syncthreads();
   if (warp == 0) {
@@ -164,11 +231,26 @@ __global__ void __launch_bounds__(kUniqueThreads)
   }
   __syncthreads();
   uint32_t pos = sb + (E[tile] - E[first]) + s_warp[warp];
+  if (vec) {
 #pragma unroll
-  for (int i = 0; i < kUniqueKpt; ++i) {
-    const uint32_t dst = pos + __popc(heads[i] & lanemask_lt());
-    if (((heads[i] >> lane) & 1u) && dst < n) out[dst] = keys[i];
-    pos += __popc(heads[i]);
+    for (int j = 0; j < NVEC; ++j) {
+      const uint32_t c = uint32_t(__popc(heads[j]));
+      const uint32_t inc = warp_inclusive_scan(c);
+      uint32_t dst = pos + inc - c;
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        if (((heads[j] >> e) & 1u) && dst < n) out[dst] = keys[j * V + e];
+        dst += (heads[j] >> e) & 1u;
+      }
+      pos += __shfl_sync(0xffffffffu, inc, 31);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kUniqueKpt; ++i) {
+      const uint32_t dst = pos + __popc(heads[i] & lanemask_lt());
+      if (((heads[i] >> lane) & 1u) && dst < n) out[dst] = keys[i];
+      pos += __popc(heads[i]);
+    }
   }
 }
 
