@@ -47,7 +47,7 @@ struct rw_tree_batch {
   uint32_t* d_class_toff = nullptr;                  // [kMaxSortClasses][n_clouds + 1]
 
   void* d_tmp_keys = nullptr;
-  uint32_t* d_tree_far = nullptr;  // radix-tree far-search list
+  uint32_t* d_tree_far = nullptr;  // far lists of the radix tree, then of the octree
   uint32_t tree_far_cap = 0;
   void* d_zero = nullptr;
   size_t zero_bytes = 0;
@@ -281,7 +281,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   cudaError_t e = cudaMalloc(&b->d_tables, (8 + rwt::kMaxSortClasses) * tab * 4);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tmp_keys, ks * total);
   b->tree_far_cap = b->tree_tiles * rwt::kTreeFarPerTile;
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tree_far, size_t(b->tree_far_cap) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_tree_far, size_t(b->tree_far_cap) * 16);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_zero, b->zero_bytes);
   if (e == cudaSuccess) e = cudaMallocHost(&b->h_results, (3 * size_t(n_clouds) + 4) * 4);
   if (e != cudaSuccess) {

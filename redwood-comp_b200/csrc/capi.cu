@@ -220,7 +220,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
   cudaError_t e = cudaMalloc(&im->d_zero, im->zero_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&im->d_tmp_keys, key_size(key_bits) * n_input);
   im->tree_far_cap = rwt::div_up(n_input, rwt::kTreeTile) * rwt::kTreeFarPerTile;
-  if (e == cudaSuccess) e = cudaMalloc(&im->d_tree_far, size_t(im->tree_far_cap) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&im->d_tree_far, size_t(im->tree_far_cap) * 16);
   if (e == cudaSuccess) e = cudaMallocHost(&im->h_status, sizeof(rwt::DevStatus));
   if (e != cudaSuccess) {
     rw_tree_im_storage_destroy(im);

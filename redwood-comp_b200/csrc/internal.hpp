@@ -26,8 +26,8 @@ struct rw_tree_im_storage {
   uint32_t sort_tiles = 0;  // tiles per pass at n_cap
 
   void* d_tmp_keys = nullptr;  // [n_cap] ping-pong buffer of the sort
-  uint32_t* d_tree_far = nullptr;  // radix-tree gaps left to the far search
-  uint32_t tree_far_cap = 0;       // entries (two words each)
+  uint32_t* d_tree_far = nullptr;  // far lists of the radix tree, then of the octree
+  uint32_t tree_far_cap = 0;       // entries (16 bytes each)
 
   // zero region
   void* d_zero = nullptr;
@@ -113,8 +113,8 @@ struct Scratch {
   uint32_t* scan_desc = nullptr;
   uint32_t* tile_ctr = nullptr;
   DevStatus* status = nullptr;
-  // [tree_far_cap][2]: radix-tree gaps left to the far search (gap, segment),
-  // then the octree's far links (node, segment)
+  // tree_far_cap entries of 16 bytes: radix-tree gaps left to the far search
+  // (gap, segment: 8 bytes each), then the octree's far links (16 bytes each)
   uint32_t* tree_far = nullptr;
   uint32_t tree_far_cap = 0;
 };

@@ -35,8 +35,11 @@ __global__ void __launch_bounds__(256)
                 TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
                 float inv_range, uint32_t* __restrict__ ghist, int passes) {
   constexpr int RADIX = 1 << D;
-  extern __shared__ uint32_t s_hist[];  // [passes][RADIX] when HIST
-  const int nh = passes * RADIX;
+  // the sort's passes: ceil(code bits / D), as the storage computes them
+  constexpr int P = (KeyTraits<K>::kCodeBits + D - 1) / D;
+  extern __shared__ uint32_t s_hist[];  // [P][RADIX] when HIST
+  const int nh = P * RADIX;
+  (void)passes;
   if (HIST) {
     for (int i = threadIdx.x; i < nh; i += blockDim.x) s_hist[i] = 0;
     __syncthreads();
@@ -62,18 +65,45 @@ __global__ void __launch_bounds__(256)
     const uint32_t sb = seg_begin(seg, c);
     const uint32_t lo = sb + (t - first) * kPointTile;
     const uint32_t hi = min(lo + kPointTile, sb + seg_size(seg, c));
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      K k;
-      if (ENCODE) {
-        const float4 p = __ldcs(pts + i);
-        k = encode<K, POW2>(p.x, p.y, p.z, min_coord, range, inv_range);
-        keys[i] = k;
-      } else {
-        k = keys[i];
-      }
+    auto count = [&](K k) {
       if (HIST) {
-        for (int ps = 0; ps < passes; ++ps)
+#pragma unroll
+        for (int ps = 0; ps < P; ++ps)
           atomicAdd(&s_hist[ps * RADIX + int((k >> (ps * D)) & K(RADIX - 1))], 1u);
+      }
+    };
+    if (hi - lo == kPointTile) {
+      // full tile: four loads in flight per thread before any is used
+      static_assert(kPointTile % (4 * 256) == 0, "whole rounds of four points per thread");
+      for (uint32_t i = lo + threadIdx.x; i < hi; i += 4 * 256) {
+        K k[4];
+        if (ENCODE) {
+          float4 p[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) p[u] = __ldcs(pts + i + 256u * u);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            k[u] = encode<K, POW2>(p[u].x, p[u].y, p[u].z, min_coord, range, inv_range);
+            keys[i + 256u * u] = k[u];
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) k[u] = keys[i + 256u * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) count(k[u]);
+      }
+    } else {
+      for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        K k;
+        if (ENCODE) {
+          const float4 p = __ldcs(pts + i);
+          k = encode<K, POW2>(p.x, p.y, p.z, min_coord, range, inv_range);
+          keys[i] = k;
+        } else {
+          k = keys[i];
+        }
+        count(k);
       }
     }
   }
@@ -296,6 +326,7 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
   const uint32_t ctas = std::max(1u, std::min<uint32_t>(tiles, uint32_t(sc.num_sms) * 8));
   const uint32_t per = div_up(tiles, ctas);
   const uint32_t grid = div_up(tiles, per);
+  if (hist && sc.passes != (KeyTraits<K>::kCodeBits + D - 1) / D) return cudaErrorInvalidValue;
   const size_t smem = hist ? size_t(sc.passes) * (1u << D) * 4 : 0;
   K* keys = static_cast<K*>(b.keys);
   const float inv = pow2_reciprocal(b.range);

@@ -911,6 +911,14 @@ __device__ __forceinline__ void link_global(const K* __restrict__ codes,
   }
 }
 
+// A far link (16 bytes): segment, node, kind << 30 | counter << 3 | slot,
+// link value.  kFarFromParent: the walk starts at parents[node] (node = the
+// linking node); kFarFromStep: node is the last ancestor reached inside the
+// tile, count 0, the walk continues at parents[node] with counter + 1;
+// kFarFinal: node is the ancestor whose row takes the link.  kFarLocal is
+// used inside k_octree only.
+constexpr uint32_t kFarFromParent = 0, kFarFromStep = 1, kFarFinal = 2, kFarLocal = 3;
+
 // Stage 7 in one pass over a tile of radix-tree nodes (func_octree.hpp:28-112).
 //
 // Rows [off[i], off[i] + cnt[i]) belong to node i (i >= 1); the offsets are
@@ -1068,54 +1076,71 @@ __global__ void __launch_bounds__(kOctThreads)
   };
 
   // links, from the chain top rows; the walk of link_parent over the tile's
-  // counts and parents.  A walk that leaves the tile or ends on a node
-  // without rows, and a value that does not fit 16 bits, go to the far list
-  // (which repeats the whole walk in global memory and merges with
-  // atomics).  Several links may name one slot (the reference keeps the
-  // last, the largest value): the 16-bit maximum is taken with
-  // compare-and-swap on the slot's word.
+  // counts and parents.  A walk that leaves the tile, ends on a node without
+  // rows or gives up, and a value that does not fit 16 bits, go to the far
+  // list with the walk's state (FarLink), where k_octree_far_links finishes
+  // the walk in global memory and merges with atomics.  Several links may
+  // name one slot (the reference keeps the last, the largest value): the
+  // 16-bit maximum is taken with compare-and-swap on the slot's word.
   for (int r = tid; rbase + r < rend; r += kOctThreads) {
     const int p = rbase + r;
     const int t = owner_of(p);
     if (r < kRowCap) s_owner[r] = uint16_t(t);
     if (p != s_off[t + 1] - 1) continue;  // not the top row of its chain
-    const uint32_t w0 = s_node[t];
-    int rp = int(w0 & 0xfffu), counter = 0;
-    bool local = rp != 0xfff;
-    uint32_t w = 0;
-    while (local) {
-      w = s_node[rp];
-      if (w >> 12) break;
-      if ((w & 0xfffu) == 0xfffu || ++counter > 30) local = false;
-      rp = int(w & 0xfffu);
+    const int level = int(s_level[t]) - (p - s_off[t]);  // the top row's level
+    const int slot = int((s_code[t] >> (B - 3 * level)) & K(7));
+    int rp = int(s_node[t] & 0xfffu), counter = 0, x = t;
+    uint32_t kind = kFarFromParent;
+    if (rp != 0xfff) {
+      for (;;) {
+        const uint32_t w = s_node[rp];
+        if (w >> 12) {
+          kind = (w >> 12) == 1 ? kFarLocal : kFarFinal;
+          break;
+        }
+        const int nx = int(w & 0xfffu);
+        if (nx == 0xfff) {  // the parent lies outside the tile
+          kind = kFarFromStep;
+          x = rp;
+          break;
+        }
+        rp = nx;
+        if (++counter > 30) {
+          kind = kFarFinal;
+          break;
+        }
+      }
     }
-    if (local && (w >> 12) == 1 && r < 0xffff) {
-      const int level = int(s_level[t]) - (p - s_off[t]);  // the top row's level
-      const int slot = int((s_code[t] >> (B - 3 * level)) & K(7));
-      uint32_t* wp = reinterpret_cast<uint32_t*>(&s_child[rp]) + (slot >> 1);
-      const int sh = 16 * (slot & 1);
-      const uint32_t rel = uint32_t(r) + 1u;  // the link value is p itself
-      uint32_t cur = *reinterpret_cast<volatile uint32_t*>(wp);
+    if (kind == kFarLocal) {
       bool done = false;
-      for (int tries = 0; tries < 64 && !done; ++tries) {  // each failure is another's success
-        if (((cur >> sh) & 0xffffu) >= rel) {
-          done = true;
-        } else {
-          const uint32_t nv = (cur & ~(0xffffu << sh)) | (rel << sh);
-          const uint32_t prev = atomicCAS(wp, cur, nv);
-          done = prev == cur;
-          cur = prev;
+      if (r < 0xffff) {
+        uint32_t* wp = reinterpret_cast<uint32_t*>(&s_child[rp]) + (slot >> 1);
+        const int sh = 16 * (slot & 1);
+        const uint32_t rel = uint32_t(r) + 1u;  // the link value is p itself
+        uint32_t cur = *reinterpret_cast<volatile uint32_t*>(wp);
+        for (int tries = 0; tries < 64 && !done; ++tries) {  // each failure is another's success
+          if (((cur >> sh) & 0xffffu) >= rel) {
+            done = true;
+          } else {
+            const uint32_t nv = (cur & ~(0xffffu << sh)) | (rel << sh);
+            const uint32_t prev = atomicCAS(wp, cur, nv);
+            done = prev == cur;
+            cur = prev;
+          }
         }
       }
       if (done) {
         atomicOr(&s_cmask[rp >> 2], 1u << (slot + 8 * (rp & 3)));
         continue;
       }
+      kind = kFarFinal;
     }
     const uint32_t at = atomicAdd(far_n, 1u);
     if (at < far_cap) {
-      far[2 * at] = uint32_t(tile0 + t);
-      far[2 * at + 1] = c;
+      const int node = kind == kFarFinal ? tile0 + rp : tile0 + x;
+      reinterpret_cast<uint4*>(far)[at] =
+          make_uint4(c, uint32_t(node), kind << 30 | uint32_t(counter) << 3 | uint32_t(slot),
+                     uint32_t(p));
     }
   }
   __syncthreads();
@@ -1212,15 +1237,33 @@ __global__ void __launch_bounds__(256)
   if (count <= far_cap) {
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
          w += gridDim.x * blockDim.x) {
-      const int i = int(far[2 * w]);
-      const uint32_t c = far[2 * w + 1];
+      const uint4 f = reinterpret_cast<const uint4*>(far)[w];
+      const uint32_t c = f.x, kind = f.z >> 30, slot = f.z & 7u;
       const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
       if (!os.ok) continue;
       const uint32_t sb = seg_begin(seg, c);
-      const int rp = link_parent(parents_all + sb, ec_all + sb, i, os.n);
-      if (rp < 0) continue;
-      link_global<K>(codes_all + sb, prefix_all + sb, off_all + sb, i, ec_all[sb + i], rp,
-                     os, o);
+      const int32_t* parents = parents_all + sb;
+      const int32_t* ec = ec_all + sb;
+      const int n = os.n;
+      int rp = int(f.y);
+      if (kind != kFarFinal) {  // the rest of link_parent's walk
+        int counter = int((f.z >> 3) & 31u);
+        rp = parents[rp];
+        if (uint32_t(rp) >= uint32_t(n)) continue;
+        bool stop = kind == kFarFromStep && ++counter > 30;
+        while (!stop && ec[rp] == 0) {
+          rp = parents[rp];
+          if (uint32_t(rp) >= uint32_t(n)) break;
+          stop = ++counter > 30;
+        }
+        if (uint32_t(rp) >= uint32_t(n)) continue;
+      }
+      const int oct_parent = off_all[sb + uint32_t(rp)];
+      if (uint32_t(oct_parent) < os.cap) {
+        const size_t r = size_t(os.row0) + uint32_t(oct_parent);
+        atomicMax(o.children + 8 * r + slot, int32_t(f.w));
+        atomicOr(o.node_mask + r, 1 << slot);
+      }
     }
     return;
   }
