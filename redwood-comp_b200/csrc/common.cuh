@@ -47,6 +47,35 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Programmatic dependent launch.  Every kernel of the pipeline starts with
+// pdl_enter(): it waits until the grid before it in the stream has completed
+// and its writes are visible (a no-op when the kernel was launched without
+// the attribute), then lets the next grid be scheduled, so that its blocks
+// take the SM slots this grid's last wave frees instead of waiting for a
+// fresh launch.  Nothing is read or written before the wait.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches a kernel that begins with pdl_enter() with programmatic stream
+// serialization; errors are reported as by a <<<>>> launch.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

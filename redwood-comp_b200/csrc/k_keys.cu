@@ -34,6 +34,7 @@ __global__ void __launch_bounds__(256)
     k_keys_pass(const float4* __restrict__ pts, K* __restrict__ keys, SegTable seg,
                 TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
                 float inv_range, uint32_t* __restrict__ ghist, int passes) {
+  pdl_enter();
   constexpr int RADIX = 1 << D;
   // the sort's passes: ceil(code bits / D), as the storage computes them
   constexpr int P = (KeyTraits<K>::kCodeBits + D - 1) / D;
@@ -119,6 +120,7 @@ template <int D>
 __global__ void __launch_bounds__(256)
     k_sort_init(const uint32_t* __restrict__ ghist, uint32_t* __restrict__ desc,
                 SegTable seg, TileMap map, int passes, uint32_t rows_per_pass) {
+  pdl_enter();
   constexpr int RADIX = 1 << D;
   constexpr int R = (RADIX + 255) / 256;
   static_assert(R * 256 >= RADIX, "every digit needs an offset");
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
               uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
+  pdl_enter();
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
   constexpr int RADIX = C::RADIX, NW = C::NW, TILE = C::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -335,7 +338,7 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
     auto kern = inv != 0.0f ? k_keys_pass<K, D, H, E, true> : k_keys_pass<K, D, H, E, false>; \
     if (smem > 48 * 1024)                                                            \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-    kern<<<grid, 256, smem, s>>>(b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
+    launch_pdl(kern, grid, 256, smem, s, b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
                                  b.range, inv, sc.ghist, sc.passes);                 \
   } while (0)
   if (encode && hist) RWT_KEYS_LAUNCH(true, true);
@@ -352,7 +355,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   auto kern = k_binning<K, D, THREADS, KPT, RANK, MINB>;
   const uint32_t tiles = pl.sort_map.n_tiles;
   if (tiles + pl.seg.count > sc.sort_rows) return cudaErrorInvalidValue;
-  k_sort_init<D><<<pl.seg.count * sc.passes, 256, 0, s>>>(sc.ghist, sc.sort_desc, pl.seg,
+  launch_pdl(k_sort_init<D>, pl.seg.count * sc.passes, 256, 0, s, sc.ghist, sc.sort_desc, pl.seg,
                                                           pl.sort_map, sc.passes, sc.sort_rows);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -366,7 +369,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   for (int p = 0; p < sc.passes; ++p) {
     K* dst = ((sc.passes - 1 - p) % 2 == 0) ? alt : tmp;
     if (tiles)
-      kern<<<tiles, THREADS, C::kSmem, s>>>(
+      launch_pdl(kern, tiles, THREADS, C::kSmem, s, 
           src, dst, pl.seg, pl.sort_map, p * D,
           sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
           sc.tile_ctr + kCtrSortBase + p, sc.status);

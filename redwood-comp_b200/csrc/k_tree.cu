@@ -46,6 +46,7 @@ namespace rwt {
 __global__ void __launch_bounds__(1024)
     k_tile_scan(uint32_t* __restrict__ E, uint32_t tiles, SegTable seg, TileMap map,
                 uint32_t* __restrict__ seg_total) {
+  pdl_enter();
   __shared__ uint32_t s_warp[33];
   constexpr int R = 16;  // 16,384 tiles per round
   uint32_t carry = 0;
@@ -171,6 +172,7 @@ template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
     k_unique_count(const K* __restrict__ sorted, SegTable seg, TileMap map,
                    uint32_t* __restrict__ E) {
+  pdl_enter();
   constexpr int NW = kUniqueThreads / 32;
   __shared__ uint32_t s_warp[NW];
   const uint32_t tile = blockIdx.x, lane = lane_id(), warp = threadIdx.x >> 5;
@@ -201,6 +203,7 @@ template <typename K>
 __global__ void __launch_bounds__(kUniqueThreads)
     k_unique_write(const K* __restrict__ sorted, K* __restrict__ out, SegTable seg, TileMap map,
                    const uint32_t* __restrict__ E) {
+  pdl_enter();
   constexpr int NW = kUniqueThreads / 32;
   __shared__ uint32_t s_warp[NW];
   const uint32_t tile = blockIdx.x, lane = lane_id(), warp = threadIdx.x >> 5;
@@ -502,6 +505,7 @@ __global__ void __launch_bounds__(kTreeThreads)
                  uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
                  int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
                  uint32_t* __restrict__ far, uint32_t far_cap, uint32_t* __restrict__ far_n) {
+  pdl_enter();
   using C = AnsvCfg<K>;
   constexpr int NV = C::NV, VB = C::VB, NW = kTreeThreads / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -688,6 +692,7 @@ __global__ void __launch_bounds__(256)
                      uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
                      uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
                      int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
+  pdl_enter();
   const uint32_t count = min(*far_n, far_cap);
   const uint32_t warps = gridDim.x * (blockDim.x / 32);
   for (uint32_t w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w < count; w += warps) {
@@ -717,6 +722,7 @@ __global__ void __launch_bounds__(256)
     k_edge_count(const uint8_t* __restrict__ prefix_n, const int32_t* __restrict__ parents,
                  int32_t* __restrict__ ec, SegTable seg, TileMap map,
                  const uint32_t* __restrict__ n_unique) {
+  pdl_enter();
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
   const uint32_t nu = n_unique[c];
@@ -772,6 +778,7 @@ __device__ __forceinline__ void scan_load(const int32_t* ec, uint32_t first, uin
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_reduce(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
                   const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E) {
+  pdl_enter();
   constexpr int NW = kScanThreads / 32;
   __shared__ uint32_t s_warp[NW];
   const uint32_t tile = blockIdx.x;
@@ -799,6 +806,7 @@ __global__ void __launch_bounds__(kScanThreads)
     k_scan_write(const int32_t* __restrict__ ec_all, int32_t* __restrict__ off_all,
                  SegTable seg, TileMap map, const uint32_t* __restrict__ n_unique,
                  const uint32_t* __restrict__ E) {
+  pdl_enter();
   __shared__ uint32_t s_warp[kScanThreads / 32 + 1];
   const uint32_t tile = blockIdx.x;
   uint32_t c, firstt, n, j;
@@ -956,6 +964,7 @@ __global__ void __launch_bounds__(kOctThreads)
              const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
              float min_coord, float range, OctOut o, uint32_t* __restrict__ far,
              uint32_t far_cap, uint32_t* __restrict__ far_n) {
+  pdl_enter();
   constexpr int B = KeyTraits<K>::kCodeBits;
   constexpr int kTile = int(kOctTile);
   constexpr int kRowCap = 2 * kTile;  // rows whose owner is kept
@@ -1190,6 +1199,7 @@ __global__ void __launch_bounds__(kOctThreads)
 __global__ void __launch_bounds__(kOctThreads)
     k_node_sums(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
                 const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E) {
+  pdl_enter();
   constexpr int kPer = int(kOctTile) / 64;  // nodes per thread
   static_assert(kOctThreads == 256 && kPer % 4 == 0, "four tiles of 64 threads");
   __shared__ uint32_t s_warp[kOctThreads / 32];
@@ -1233,6 +1243,7 @@ __global__ void __launch_bounds__(256)
                        const uint32_t* __restrict__ n_octree, int32_t* __restrict__ seg_err,
                        OctOut o, const uint32_t* __restrict__ far, uint32_t far_cap,
                        const uint32_t* __restrict__ far_n) {
+  pdl_enter();
   const uint32_t count = *far_n;
   if (count <= far_cap) {
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
@@ -1300,10 +1311,10 @@ cudaError_t unique_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   const uint32_t tiles = pl.unique_map.n_tiles;
   if (!tiles) return cudaSuccess;
   const K* sorted = static_cast<const K*>(b.alt);
-  k_unique_count<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, pl.seg, pl.unique_map,
+  launch_pdl(k_unique_count<K>, tiles, kUniqueThreads, 0, s, sorted, pl.seg, pl.unique_map,
                                                      sc.unique_desc);
-  k_tile_scan<<<1, 1024, 0, s>>>(sc.unique_desc, tiles, pl.seg, pl.unique_map, pl.n_unique);
-  k_unique_write<K><<<tiles, kUniqueThreads, 0, s>>>(sorted, static_cast<K*>(b.keys), pl.seg,
+  launch_pdl(k_tile_scan, 1, 1024, 0, s, sc.unique_desc, tiles, pl.seg, pl.unique_map, pl.n_unique);
+  launch_pdl(k_unique_write<K>, tiles, kUniqueThreads, 0, s, sorted, static_cast<K*>(b.keys), pl.seg,
                                                      pl.unique_map, sc.unique_desc);
   return cudaGetLastError();
 }
@@ -1321,17 +1332,17 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
   uint32_t* far_n = sc.tile_ctr + kCtrTree;
   const int far_blocks = std::max(1, sc.num_sms * 8);
   if (edges) {
-    k_radix_tree<K, true><<<tiles, kTreeThreads, smem, s>>>(
+    launch_pdl(k_radix_tree<K, true>, tiles, kTreeThreads, smem, s, 
         codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
         b.parents, b.edge_count, sc.tree_far, sc.tree_far_cap, far_n);
-    k_radix_tree_far<K, true><<<far_blocks, 256, 0, s>>>(
+    launch_pdl(k_radix_tree_far<K, true>, far_blocks, 256, 0, s, 
         codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
         b.hr, b.lc, b.parents, b.edge_count);
   } else {
-    k_radix_tree<K, false><<<tiles, kTreeThreads, smem, s>>>(
+    launch_pdl(k_radix_tree<K, false>, tiles, kTreeThreads, smem, s, 
         codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
         b.parents, nullptr, sc.tree_far, sc.tree_far_cap, far_n);
-    k_radix_tree_far<K, false><<<far_blocks, 256, 0, s>>>(
+    launch_pdl(k_radix_tree_far<K, false>, far_blocks, 256, 0, s, 
         codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
         b.hr, b.lc, b.parents, nullptr);
   }
@@ -1346,16 +1357,19 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   const K* codes = static_cast<const K*>(b.keys);
   const uint32_t tiles = pl.node_map.n_tiles;
   uint32_t* far_n = sc.tile_ctr + kCtrLinks;
-  cudaError_t e = cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
+  // the fused pipeline clears every counter when it starts; stage 7 run alone
+  // clears its own (a memset between two kernels would also end the
+  // programmatic launch chain)
+  cudaError_t e = fused_offsets ? cudaSuccess : cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   if (tiles) {
     if (fused_offsets)
-      k_octree<K, true><<<tiles, kOctThreads, 0, s>>>(
+      launch_pdl(k_octree<K, true>, tiles, kOctThreads, 0, s, 
           codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, sc.scan_desc, pl.seg,
           pl.node_map, pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o,
           sc.tree_far, sc.tree_far_cap, far_n);
     else
-      k_octree<K, false><<<tiles, kOctThreads, 0, s>>>(
+      launch_pdl(k_octree<K, false>, tiles, kOctThreads, 0, s, 
           codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, nullptr, pl.seg,
           pl.node_map, pl.n_unique, pl.n_octree, pl.seg_err, b.min_coord, b.range, o,
           sc.tree_far, sc.tree_far_cap, far_n);
@@ -1364,7 +1378,7 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
   if (tiles)
-    k_octree_far_links<K><<<std::max(1, sc.num_sms * 8), 256, 0, s>>>(
+    launch_pdl(k_octree_far_links<K>, std::max(1, sc.num_sms * 8), 256, 0, s, 
         codes, b.prefix_n, b.parents, b.edge_count, b.edge_offset, pl.seg, pl.node_map,
         pl.n_unique, pl.n_octree, pl.seg_err, o, sc.tree_far, sc.tree_far_cap, far_n);
   e = cudaGetLastError();
@@ -1404,7 +1418,7 @@ cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
                               cudaStream_t s) {
   (void)sc;
   if (!pl.node_map.n_tiles) return cudaSuccess;
-  k_edge_count<<<pl.node_map.n_tiles, kOctThreads, 0, s>>>(
+  launch_pdl(k_edge_count, pl.node_map.n_tiles, kOctThreads, 0, s, 
       b.prefix_n, b.parents, b.edge_count, pl.seg, pl.node_map, pl.n_unique);
   return cudaGetLastError();
 }
@@ -1412,10 +1426,10 @@ cudaError_t launch_edge_count(const Bufs& b, const Scratch& sc, const Plan& pl,
 cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
   const uint32_t tiles = pl.scan_map.n_tiles;
   if (!tiles) return cudaSuccess;
-  k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(b.edge_count, pl.seg, pl.scan_map, pl.n_unique,
+  launch_pdl(k_scan_reduce, tiles, kScanThreads, 0, s, b.edge_count, pl.seg, pl.scan_map, pl.n_unique,
                                                sc.scan_desc);
-  k_tile_scan<<<1, 1024, 0, s>>>(sc.scan_desc, tiles, pl.seg, pl.scan_map, pl.n_octree);
-  k_scan_write<<<tiles, kScanThreads, 0, s>>>(b.edge_count, b.edge_offset, pl.seg,
+  launch_pdl(k_tile_scan, 1, 1024, 0, s, sc.scan_desc, tiles, pl.seg, pl.scan_map, pl.n_octree);
+  launch_pdl(k_scan_write, tiles, kScanThreads, 0, s, b.edge_count, b.edge_offset, pl.seg,
                                               pl.scan_map, pl.n_unique, sc.scan_desc);
   return cudaGetLastError();
 }
@@ -1423,9 +1437,9 @@ cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, c
 cudaError_t launch_edge_sums(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
   const uint32_t tiles = pl.node_map.n_tiles;
   if (!tiles) return cudaSuccess;
-  k_node_sums<<<div_up(tiles, 4), kOctThreads, 0, s>>>(b.edge_count, pl.seg, pl.node_map,
+  launch_pdl(k_node_sums, div_up(tiles, 4), kOctThreads, 0, s, b.edge_count, pl.seg, pl.node_map,
                                                       pl.n_unique, sc.scan_desc);
-  k_tile_scan<<<1, 1024, 0, s>>>(sc.scan_desc, tiles, pl.seg, pl.node_map, pl.n_octree);
+  launch_pdl(k_tile_scan, 1, 1024, 0, s, sc.scan_desc, tiles, pl.seg, pl.node_map, pl.n_octree);
   return cudaGetLastError();
 }
 
