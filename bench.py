@@ -696,7 +696,7 @@ def main():
         "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
                               "frac": round(pipe_gbs / hbm, 4)},
         "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
-        "clocks": clocks.summary(), "gpu_launches": (12 + passes) * a.steps,
+        "clocks": clocks.summary(), "gpu_launches": (11 + passes) * a.steps,
         "forms": forms,
     }
     print(json.dumps(line), flush=True)

@@ -47,25 +47,41 @@ __global__ void __launch_bounds__(1024)
     k_tile_scan(uint32_t* __restrict__ E, uint32_t tiles, SegTable seg, TileMap map,
                 uint32_t* __restrict__ seg_total) {
   pdl_enter();
+  // rounds of 1,024 x J tiles; warp w scans its contiguous 32 x J slice with
+  // coalesced loads (J warp scans with a running carry), then one warp scans
+  // the 32 warp sums
+  constexpr int J = 16;
   __shared__ uint32_t s_warp[33];
-  constexpr int R = 16;  // 16,384 tiles per round
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   uint32_t carry = 0;
-  for (uint32_t c0 = 0; c0 < tiles; c0 += 1024 * R) {
-    const uint32_t f = c0 + threadIdx.x * R;
-    uint32_t v[R], loc = 0;
+  for (uint32_t c0 = 0; c0 < tiles; c0 += 1024u * J) {
+    const uint32_t wb = c0 + warp * 32u * J + lane;
+    uint32_t v[J];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      v[r] = f + r < tiles ? E[f + r] : 0u;
-      loc += v[r];
-    }
-    uint32_t total;
-    uint32_t run = carry + block_exclusive_scan<1024>(loc, s_warp, &total);
+    for (int j = 0; j < J; ++j) v[j] = wb + 32u * j < tiles ? E[wb + 32u * j] : 0u;
+    uint32_t run = 0;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (f + r < tiles) E[f + r] = run;
-      run += v[r];
+    for (int j = 0; j < J; ++j) {
+      const uint32_t inc = warp_inclusive_scan(v[j]);
+      const uint32_t x = v[j];
+      v[j] = run + inc - x;  // exclusive within the warp's slice
+      run += __shfl_sync(0xffffffffu, inc, 31);
     }
-    carry += total;
+    if (lane == 0) s_warp[warp] = run;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t w = s_warp[lane];
+      const uint32_t wi = warp_inclusive_scan(w);
+      s_warp[lane] = wi - w;
+      if (lane == 31) s_warp[32] = wi;
+    }
+    __syncthreads();
+    const uint32_t wofs = carry + s_warp[warp];
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (wb + 32u * j < tiles) E[wb + 32u * j] = wofs + v[j];
+    carry += s_warp[32];
+    __syncthreads();  // s_warp is reused by the next round
   }
   if (threadIdx.x == 0) E[tiles] = carry;
   __syncthreads();
