@@ -392,7 +392,7 @@ struct SortVariant {
 // The menu the autotuner chooses from (entry 0 of each key/digit width is
 // the default).
 const SortVariant kVariants[] = {
-    {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 2>},
+    {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 3>},
     {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 2>},
     {32, 8, 384, 16, kRankAtomicOr, passes_t<uint32_t, 8, 384, 16, kRankAtomicOr, 2>},
     {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 3>},
