@@ -33,14 +33,13 @@ template <typename K, int D, bool HIST, bool ENCODE, bool POW2>
 __global__ void __launch_bounds__(256)
     k_keys_pass(const float4* __restrict__ pts, K* __restrict__ keys, SegTable seg,
                 TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
-                float inv_range, uint32_t* __restrict__ ghist, int passes) {
+                float inv_range, uint32_t* __restrict__ ghist) {
   pdl_enter();
   constexpr int RADIX = 1 << D;
   // the sort's passes: ceil(code bits / D), as the storage computes them
   constexpr int P = (KeyTraits<K>::kCodeBits + D - 1) / D;
   extern __shared__ uint32_t s_hist[];  // [P][RADIX] when HIST
   const int nh = P * RADIX;
-  (void)passes;
   if (HIST) {
     for (int i = threadIdx.x; i < nh; i += blockDim.x) s_hist[i] = 0;
     __syncthreads();
@@ -339,7 +338,7 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
     if (smem > 48 * 1024)                                                            \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
     launch_pdl(kern, grid, 256, smem, s, b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
-                                 b.range, inv, sc.ghist, sc.passes);                 \
+                                 b.range, inv, sc.ghist);                            \
   } while (0)
   if (encode && hist) RWT_KEYS_LAUNCH(true, true);
   else if (encode) RWT_KEYS_LAUNCH(false, true);
