@@ -430,62 +430,59 @@ struct AnsvCfg {
                                   2 * size_t(kTreeTile) + size_t(kAnsvWin) + size_t(kAnsvChunks);
 };
 
-// Warp-cooperative searches for the nearest smaller gap of gap g beyond any
-// window: 32 probes per round (doubling distances, then 32-ary refinement), so
-// a search costs about six dependent loads.  pred(a) = delta(key a, key g) > D
-// is true from some a_min up to g; returns a_min (the node's first key).
+// Warp-cooperative search for the nearest smaller gaps of gap g beyond any
+// window, both sides in lockstep: 32 probes per side and round (doubling
+// distances, then 32-ary refinement), the two sides' loads issued together,
+// so the pair costs about as many dependent loads as the longer side.
+// Left: pred(a) = delta(key a, key g) > D is true from some a_min up to g;
+// *first_key = a_min (the node's first key).  Right: pred(b) = delta(key g+1,
+// key b) > D is true from g+1 up to some b_max <= n; *last_key = b_max.
 template <typename K>
-__device__ int coop_first_key(const K* __restrict__ codes, int g, int D) {
+__device__ void coop_node_keys(const K* __restrict__ codes, int n, int g, int D,
+                               int* first_key, int* last_key) {
   const uint32_t lane = lane_id();
-  const K cg = codes[g], lim = delta_limit<K>(D);
-  const int p = lane < 31 ? g - (1 << lane) : -1;
-  const bool f = p >= 0 && (codes[p] ^ cg) < lim;
-  const int js = __ffs(__ballot_sync(0xffffffffu, !f)) - 1;  // a false probe exists
-  int lo = max(js < 31 ? g - (1 << js) : -1, -1);                // pred(lo) false
-  int hi = js == 0 ? g : g - (1 << (js - 1));                    // pred(hi) true
-  while (hi - lo > 1) {
-    const int step = (hi - lo + 31) / 32;
-    const int q = lo + (int(lane) + 1) * step;
-    const bool in = lane < 31 && q < hi;
-    const bool t = in && (codes[q] ^ cg) < lim;
-    const uint32_t mt = __ballot_sync(0xffffffffu, t), mi = __ballot_sync(0xffffffffu, in);
-    if (mt) {
-      const int ft = __ffs(mt) - 1;
-      hi = lo + (ft + 1) * step;
-      lo = ft > 0 ? lo + ft * step : lo;
-    } else {
-      lo = lo + (32 - __clz(mi)) * step;  // the last probe in range is false
+  const K cl = codes[g], cr = codes[g + 1], lim = delta_limit<K>(D);
+  const int pl = lane < 31 ? g - (1 << lane) : -1;
+  const long long pr = lane < 31 ? (long long)g + 1 + (1ll << lane) : (long long)n + 1;
+  const bool fl = pl >= 0 && (codes[pl] ^ cl) < lim;
+  const bool fr = pr <= n && (codes[int(pr)] ^ cr) < lim;
+  const int jl = __ffs(__ballot_sync(0xffffffffu, !fl)) - 1;  // a false probe exists
+  const int jr = __ffs(__ballot_sync(0xffffffffu, !fr)) - 1;
+  int llo = max(jl < 31 ? g - (1 << jl) : -1, -1);                // pred(llo) false
+  int lhi = jl == 0 ? g : g - (1 << (jl - 1));                    // pred(lhi) true
+  int rhi = jr < 31 ? int(min((long long)g + 1 + (1ll << jr), (long long)n + 1)) : n + 1;
+  int rlo = jr == 0 ? g + 1 : g + 1 + (1 << (jr - 1));            // pred(rlo) true
+  while (lhi - llo > 1 || rhi - rlo > 1) {
+    const bool la = lhi - llo > 1, ra = rhi - rlo > 1;  // warp-uniform
+    const int ls = la ? (lhi - llo + 31) / 32 : 0, rs = ra ? (rhi - rlo + 31) / 32 : 0;
+    const int lq = llo + (int(lane) + 1) * ls, rq = rlo + (int(lane) + 1) * rs;
+    const bool lin = la && lane < 31 && lq < lhi, rin = ra && lane < 31 && rq < rhi;
+    const bool lt = lin && (codes[lq] ^ cl) < lim;
+    const bool rt = rin && (codes[rq] ^ cr) < lim;
+    const uint32_t mlt = __ballot_sync(0xffffffffu, lt), mli = __ballot_sync(0xffffffffu, lin);
+    const uint32_t mrf = __ballot_sync(0xffffffffu, rin && !rt),
+                   mri = __ballot_sync(0xffffffffu, rin);
+    if (la) {
+      if (mlt) {
+        const int ft = __ffs(mlt) - 1;
+        lhi = llo + (ft + 1) * ls;
+        llo = ft > 0 ? llo + ft * ls : llo;
+      } else {
+        llo = llo + (32 - __clz(mli)) * ls;  // the last probe in range is false
+      }
+    }
+    if (ra) {
+      if (mrf) {
+        const int ff = __ffs(mrf) - 1;
+        rhi = rlo + (ff + 1) * rs;
+        rlo = ff > 0 ? rlo + ff * rs : rlo;
+      } else {
+        rlo = rlo + (32 - __clz(mri)) * rs;  // every probe in range is true
+      }
     }
   }
-  return hi;
-}
-
-// pred(b) = delta(key g+1, key b) > D is true from g+1 up to some b_max <= n;
-// returns b_max (the node's last key).
-template <typename K>
-__device__ int coop_last_key(const K* __restrict__ codes, int n, int g, int D) {
-  const uint32_t lane = lane_id();
-  const K cg = codes[g + 1], lim = delta_limit<K>(D);
-  const long long p = lane < 31 ? (long long)g + 1 + (1ll << lane) : (long long)n + 1;
-  const bool f = p <= n && (codes[int(p)] ^ cg) < lim;
-  const int js = __ffs(__ballot_sync(0xffffffffu, !f)) - 1;
-  int hi = js < 31 ? int(min((long long)g + 1 + (1ll << js), (long long)n + 1)) : n + 1;
-  int lo = js == 0 ? g + 1 : g + 1 + (1 << (js - 1));            // pred(lo) true
-  while (hi - lo > 1) {
-    const int step = (hi - lo + 31) / 32;
-    const int q = lo + (int(lane) + 1) * step;
-    const bool in = lane < 31 && q < hi;
-    const bool t = in && (codes[q] ^ cg) < lim;
-    const uint32_t mf = __ballot_sync(0xffffffffu, in && !t), mi = __ballot_sync(0xffffffffu, in);
-    if (mf) {
-      const int ff = __ffs(mf) - 1;
-      hi = lo + (ff + 1) * step;
-      lo = ff > 0 ? lo + ff * step : lo;
-    } else {
-      lo = lo + (32 - __clz(mi)) * step;  // every probe in range is true
-    }
-  }
-  return lo;
+  *first_key = lhi;
+  *last_key = rlo;
 }
 
 // Writes the node that splits at gap g, given its nearest smaller gaps L, R
@@ -718,8 +715,10 @@ __global__ void __launch_bounds__(256)
     const int g = int(far[2 * w] - sb);
     const K* codes = codes_all + sb;
     const int D = delta(codes[g], codes[g + 1]);
-    const int L = coop_first_key<K>(codes, g, D) - 1;
-    const int R = coop_last_key<K>(codes, n, g, D);
+    int first_key, last_key;
+    coop_node_keys<K>(codes, n, g, D, &first_key, &last_key);
+    const int L = first_key - 1;
+    const int R = last_key;
     if (lane_id() == 0) {
       auto d_at = [&](int p) -> int { return delta(codes[p], codes[p + 1]); };
       const int rtd = EDGES ? delta(codes[0], codes[n]) : 0;
