@@ -56,6 +56,10 @@ def parse_args():
                    help="time only the device-resident pipeline (for profiler runs)")
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batched and learned forms in the default line")
+    # internal: time the reference's CPU path in a child process (see ref_time_isolated)
+    p.add_argument("--ref-time-child", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--ref-threads", type=int, default=0, help=argparse.SUPPRESS)
+    p.add_argument("--ref-iters", type=int, default=1, help=argparse.SUPPRESS)
     return p.parse_args()
 
 
@@ -184,27 +188,25 @@ def traffic_table():
 def run_reference(a, rank):
     if rank != 0:
         return 0
-    from oracle import RefTree, ref_available
+    from oracle import ref_available
     from __graft_entry__ import _load_package
     rw = _load_package()
     pts = make_points(rw, a.n, a.dist, a.seed)
-    if a.key_bits != 32 or not ref_available():
-        # the reference has no 64-bit path; the C restatement stands in
-        from oracle import Oracle
-        orc = Oracle()
+    note = None
+    ms = None
+    if a.key_bits == 32 and ref_available():
+        ms, cores = ref_time_isolated(a, a.seed, a.warmup + a.steps)
+        if ms is not None:
+            kind = "reference"
+            ms = ms[a.warmup:]
+        else:
+            note = cores
+    if ms is None:
+        # the reference has no 64-bit path (or failed on this cloud): the C
+        # restatement stands in
         kind, cores = "port", 1
-        for _ in range(a.warmup):
-            orc.run(pts, key_bits=a.key_bits)
-        ms = []
-        for _ in range(a.steps):
-            t0 = time.perf_counter()
-            orc.run(pts, key_bits=a.key_bits)
-            ms.append((time.perf_counter() - t0) * 1e3)
-    else:
-        ref = RefTree()
-        cores = ref.hardware_threads()
-        kind = "reference"
-        ms = list(ref.time(pts, cores, a.warmup + a.steps))[a.warmup:]
+        port_time(pts, a, a.warmup)
+        ms = port_time(pts, a, a.steps)
     t = statistics.median(ms)
     val = a.n / (t / 1e3)
     line = {
@@ -220,6 +222,8 @@ def run_reference(a, rank):
         "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if note:
+        line["cpu_baseline"]["note"] = note
     print(json.dumps(line), flush=True)
     return 0
 
@@ -470,25 +474,73 @@ def measure_learned(rw, a, n=67_108_864, reps=10):
     return info
 
 
-def cpu_baseline(rw, pts, a):
-    from oracle import RefTree, ref_available
-    if a.key_bits != 32 or not ref_available():
-        from oracle import Oracle
-        orc = Oracle()
+def ref_time_child(a):
+    """Child side of ref_time_isolated: the same seeded cloud, the reference's
+    verbatim stages 1-7 timed `--ref-iters` times; prints {"ms": [...]}."""
+    from oracle import RefTree
+    from __graft_entry__ import _load_package
+    rw = _load_package()
+    pts = make_points(rw, a.n, a.dist, a.seed)
+    ref = RefTree()
+    cores = a.ref_threads or ref.hardware_threads()
+    ms = ref.time(pts, cores, a.ref_iters)
+    print(json.dumps({"ms": [float(x) for x in ms], "cores": cores}), flush=True)
+    return 0
+
+
+def ref_time_isolated(a, seed, iters):
+    """Wall ms of `iters` runs of the reference's own CPU pipeline (oracle/_ref)
+    on the cloud make_points(n, dist, seed) gives, in a child process: the
+    reference's stage 7 writes out of bounds on some clouds (negative octree
+    offsets reach func_octree.hpp:101), which must not take this process down.
+    Returns (ms list, cores) or (None, reason)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--ref-time-child", "--n", str(a.n),
+           "--dist", a.dist, "--seed", str(seed), "--ref-iters", str(iters)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    except subprocess.TimeoutExpired:
+        return None, "the reference's CPU path did not finish in 30 minutes"
+    if r.returncode != 0:
+        how = f"signal {-r.returncode}" if r.returncode < 0 else f"exit {r.returncode}"
+        return None, (f"the reference's CPU path ended with {how} on this cloud "
+                      f"(out-of-bounds writes in its stage 7)")
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    return out["ms"], out["cores"]
+
+
+def port_time(pts, a, iters):
+    from oracle import Oracle
+    orc = Oracle()
+    ms = []
+    for _ in range(iters):
         t0 = time.perf_counter()
         orc.run(pts, key_bits=a.key_bits)
-        t = time.perf_counter() - t0
-        return {"value": a.n / t, "unit": "points/s", "cores": 1, "kind": "port",
-                "sample": f"1 run of the C restatement on the n={a.n} cloud"}
-    ref = RefTree()
-    cores = ref.hardware_threads()
-    first = ref.time(pts, cores, 1)[0]
-    iters = int(min(10, max(3, 15000.0 / max(first, 1.0))))
-    ms = ref.time(pts, cores, iters)
-    t = statistics.median(ms)
-    return {"value": a.n / (t / 1e3), "unit": "points/s", "cores": cores, "kind": "reference",
-            "sample": f"median of {iters} runs of cpu::run_stage1..7 (verbatim, "
-                      f"{cores} threads) on the same n={a.n} cloud, after 1 warm run"}
+        ms.append((time.perf_counter() - t0) * 1e3)
+    return ms
+
+
+def cpu_baseline(rw, pts, a):
+    from oracle import ref_available
+    note = None
+    if a.key_bits == 32 and ref_available():
+        first, info = ref_time_isolated(a, a.seed, 1)
+        if first is not None:
+            iters = int(min(10, max(3, 15000.0 / max(first[0], 1.0))))
+            ms, info = ref_time_isolated(a, a.seed, iters)
+            if ms is not None:
+                t = statistics.median(ms)
+                return {"value": a.n / (t / 1e3), "unit": "points/s", "cores": info,
+                        "kind": "reference",
+                        "sample": f"median of {iters} runs of cpu::run_stage1..7 (verbatim, "
+                                  f"{info} threads) on the same n={a.n} cloud, after 1 warm "
+                                  f"run"}
+        note = info  # why the reference could not be timed
+    t = port_time(pts, a, 1)[0]
+    line = {"value": a.n / (t / 1e3), "unit": "points/s", "cores": 1, "kind": "port",
+            "sample": f"1 run of the C restatement on the n={a.n} cloud"}
+    if note:
+        line["note"] = note
+    return line
 
 
 def main():
@@ -496,6 +548,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.ref_time_child:
+        return ref_time_child(a)
     if a.impl == "reference":
         return run_reference(a, rank)
 
