@@ -873,8 +873,9 @@ struct OctOut {
 
 struct OctSeg {
   uint32_t row0, cap, m;
-  int n;  // radix-tree nodes
-  bool ok;
+  int n;        // radix-tree nodes
+  bool counts;  // the counts are valid (the edge offsets can be made)
+  bool ok;      // ... and the octree fits its rows
 };
 
 // The segment's octree rows and counts; reports a too small octree.
@@ -890,6 +891,7 @@ __device__ __forceinline__ OctSeg oct_segment(const SegTable& seg, const OctOut&
   r.m = *reinterpret_cast<const volatile uint32_t*>(n_octree + c);
   r.row0 = o.oct_off ? o.oct_off[c] : 0u;
   r.cap = o.oct_off ? o.oct_off[c + 1] - o.oct_off[c] : o.capacity;
+  r.counts = true;
   if (uint64_t(r.m) + 1 > r.cap) {
     if (report) seg_error(seg_err, c, RW_ERR_CAPACITY);
     r.ok = false;
@@ -1003,7 +1005,9 @@ __global__ void __launch_bounds__(kOctThreads)
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
   const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c,
                                 blockIdx.x == first && threadIdx.x == 0);
-  if (!os.ok) return;
+  // with OFFS a too small octree still gets its edge offsets (stage 6's
+  // output), as when stage 6 runs on its own
+  if (OFFS ? !os.counts : !os.ok) return;
   const int n = os.n;
   const int tile0 = int(blockIdx.x - first) * kTile;
   if (tile0 >= n) return;
@@ -1061,6 +1065,7 @@ __global__ void __launch_bounds__(kOctThreads)
     }
     rows_end = base + s_wsum[32];
   }
+  if (!os.ok) return;  // the whole block: no octree row is written
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int t = tid + q * kOctThreads;

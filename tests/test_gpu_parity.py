@@ -157,6 +157,45 @@ def test_degenerate_and_counts(rw):
     assert app.get_n_unique() > 900
 
 
+@pytest.mark.gpu
+def test_capacity_error_keeps_stages_1_to_6(rw, oracle):
+    """An octree too large for its rows stops stage 7 with RW_ERR_CAPACITY
+    (the reference would write past the buffer); the fused pipeline still
+    leaves every output of stages 1-6 exact, the edge offsets included, as a
+    stage-by-stage run does."""
+    n = 20000
+    pts = cloud(rw, n, "uniform", 11)
+    want = oracle.run(pts)
+    assert want.status == ORC_OK
+    u, b = want.n_unique, want.n_brt_nodes
+    for run in ("fused", "stagewise"):
+        app = rw.AppData(n, 32, points=pts, octree_ratio=0.01)
+        im = rw.ImStorage(n, 32)
+        with pytest.raises(rw.RwTreeError) as e:
+            if run == "fused":
+                rw.run_pipeline(app, im)
+            else:
+                for k in range(1, 8):
+                    getattr(rw, f"run_stage{k}")(app, im)
+        assert e.value.code == rw.RW_ERR_CAPACITY, run
+        got = {
+            "sorted_keys": app.u_morton_keys_alt.cpu().numpy(),
+            "unique_keys": app.u_morton_keys[:u].cpu().numpy(),
+            "prefix_n": app.brt_prefix_n[:b].cpu().numpy(),
+            "parents": app.brt_parents[:b].cpu().numpy(),
+            "left_child": app.brt_left_child[:b].cpu().numpy(),
+            "edge_count": app.u_edge_count[:b].cpu().numpy(),
+            "edge_offset": app.u_edge_offset[:b].cpu().numpy(),
+        }
+        ref = {"sorted_keys": want.sorted_keys, "unique_keys": want.unique_keys[:u],
+               "prefix_n": want.prefix_n[:b], "parents": want.parents[:b],
+               "left_child": want.left_child[:b], "edge_count": want.edge_count[:b],
+               "edge_offset": want.edge_offset[:b]}
+        for k, v in ref.items():
+            assert np.ascontiguousarray(got[k]).view(np.uint8).tobytes() == \
+                np.ascontiguousarray(v).view(np.uint8).tobytes(), (run, k)
+
+
 def test_stage_order_enforced(rw):
     n = 1000
     app = rw.AppData(n, 32, points=cloud(rw, n, "uniform", 4))
