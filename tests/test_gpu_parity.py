@@ -120,6 +120,27 @@ def test_buffers_reused_across_inputs(rw, oracle):
     assert_same(app.results(), oracle.run(a), "reuse stagewise")
 
 
+def test_pipeline_replayed_from_a_cuda_graph(rw, oracle):
+    """rw_tree_pipeline_enqueue captured once into a CUDA graph (the kernels use
+    programmatic dependent launch) and replayed on new clouds in the same
+    buffers: every replay exact, counts read by pipeline_finish."""
+    import torch
+    n = 100000
+    app = rw.AppData(n, 32, points=cloud(rw, n, "uniform", 21))
+    im = rw.ImStorage(n, 32)
+    rw.run_pipeline(app, im)  # first run outside the capture
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rw.pipeline_enqueue(app, im)
+    for kind, seed in (("gauss", 22), ("uniform", 23), ("appdata", 24)):
+        pts = cloud(rw, n, kind, seed)
+        app.set_points(pts)
+        g.replay()
+        rw.pipeline_finish(app, im)
+        assert_same(app.results(), oracle.run(pts), f"graph replay {kind}")
+    del g
+
+
 def test_sort_stage_matches_numpy(rw):
     """Stage 2 alone on adversarial key sets."""
     import torch
