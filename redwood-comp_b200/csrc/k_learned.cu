@@ -87,6 +87,7 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
 // 1. stratified sample: one key from each of kSample equal strata
 __global__ void k_sample(const uint32_t* __restrict__ keys, uint32_t n,
                          uint32_t* __restrict__ sample) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kSample) return;
   const uint64_t lo = (uint64_t(i) * n) / kSample, hi = (uint64_t(i + 1) * n) / kSample;
@@ -141,6 +142,7 @@ __device__ __forceinline__ uint32_t boundary_from_output(const uint32_t* __restr
 __global__ void __launch_bounds__(256)
     k_boundaries(const uint32_t* __restrict__ sorted_sample, uint32_t group,
                  uint32_t* __restrict__ bounds, float* __restrict__ features) {
+  pdl_enter();
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= kBounds) return;
   const uint32_t c = (j + 1) * kSpacing;  // sample rank of the ideal boundary
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(256)
 // prefix maximum over the boundaries (one block): non-decreasing boundaries
 // are what makes "bucket = number of boundaries <= key" order-preserving
 __global__ void __launch_bounds__(1024) k_bounds_monotone(uint32_t* __restrict__ bounds) {
+  pdl_enter();
   __shared__ uint32_t s_warp[32];
   constexpr int R = kBuckets / 1024;
   const int first = threadIdx.x * R;
@@ -229,6 +232,7 @@ constexpr uint32_t kBpPerCta = kBpGroup * kBpRounds;
 __global__ void __launch_bounds__(kBpThreads)
     k_boundaries_mlp(const uint32_t* __restrict__ sorted_sample, const float* __restrict__ params,
                      uint32_t group, uint32_t* __restrict__ bounds) {
+  pdl_enter();
   __shared__ float s_w1[kMlpHidden * kMlpIn], s_w2[kMlpHidden * kMlpHidden], s_w3[kMlpHidden],
       s_b1[kMlpHidden], s_b2[kMlpHidden];
   __shared__ float s_x[kBpGroup][kMlpIn], s_h1[kBpGroup][kMlpHidden], s_part[kBpGroup][2];
@@ -298,6 +302,7 @@ __global__ void __launch_bounds__(kSpThreads, 2)
             uint32_t src_cap, uint32_t tiles_per_seg, uint32_t root0,
             const uint32_t* __restrict__ bounds, uint32_t* __restrict__ cursor,
             uint32_t* __restrict__ region, uint32_t cap) {
+  pdl_enter();
   using C = SplitCfg<LEVELS>;
   constexpr uint32_t BINS = C::BINS;
   static_assert(BINS <= 256, "bins are kept in bytes");
@@ -408,6 +413,7 @@ __global__ void __launch_bounds__(1024)
                   const uint32_t* __restrict__ super_counts, uint32_t scap,
                   uint32_t* __restrict__ offsets, uint32_t* __restrict__ order,
                   LearnedPlan* __restrict__ plan) {
+  pdl_enter();
   __shared__ uint32_t s_warp[33];
   __shared__ uint32_t s_front, s_back;
   constexpr int R = kBuckets / 1024;
@@ -705,6 +711,7 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     k_bucket_sort(uint32_t* __restrict__ region, uint32_t cap, const uint32_t* __restrict__ counts,
                   const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ order,
                   uint32_t* __restrict__ out) {
+  pdl_enter();
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t bk = order[blockIdx.x];
   const uint32_t cnt = counts[bk];
@@ -765,18 +772,18 @@ int boundaries(rw_tree_learned* L, bool mlp, bool features, cudaStream_t s) {
   if (mlp && !L->has_params) return RW_ERR_NOT_READY;
   const uint32_t blocks = (rwt::kBounds + 255) / 256;
   if (features) {  // training data (the per-boundary kernel writes the inputs)
-    rwt::k_boundaries<<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->group, L->d_bounds,
+    rwt::launch_pdl(rwt::k_boundaries, blocks, 256, 0, s, L->d_sample_sorted, L->group, L->d_bounds,
                                              L->d_features);
     RWL_CUDA(cudaGetLastError());
   }
   if (mlp) {
     const uint32_t ctas = (rwt::kBounds + rwt::kBpPerCta - 1) / rwt::kBpPerCta;
-    rwt::k_boundaries_mlp<<<ctas, rwt::kBpThreads, 0, s>>>(L->d_sample_sorted, L->d_params,
+    rwt::launch_pdl(rwt::k_boundaries_mlp, ctas, rwt::kBpThreads, 0, s, L->d_sample_sorted, L->d_params,
                                                           L->group, L->d_bounds);
     RWL_CUDA(cudaGetLastError());
-    rwt::k_bounds_monotone<<<1, 1024, 0, s>>>(L->d_bounds);
+    rwt::launch_pdl(rwt::k_bounds_monotone, 1, 1024, 0, s, L->d_bounds);
   } else if (!features) {
-    rwt::k_boundaries<<<blocks, 256, 0, s>>>(L->d_sample_sorted, L->group, L->d_bounds,
+    rwt::launch_pdl(rwt::k_boundaries, blocks, 256, 0, s, L->d_sample_sorted, L->group, L->d_bounds,
                                              nullptr);
   }
   RWL_CUDA(cudaGetLastError());
@@ -785,7 +792,7 @@ int boundaries(rw_tree_learned* L, bool mlp, bool features, cudaStream_t s) {
 
 int front_half(rw_tree_learned* L, const uint32_t* keys, uint32_t n, bool mlp, bool features,
                cudaStream_t s) {
-  rwt::k_sample<<<rwt::kSample / 256, 256, 0, s>>>(keys, n, L->d_sample);
+  rwt::launch_pdl(rwt::k_sample, rwt::kSample / 256, 256, 0, s, keys, n, L->d_sample);
   RWL_CUDA(cudaGetLastError());
   if (int rc = sort_sample(L, s)) return rc;
   return boundaries(L, mlp, features, s);
@@ -799,15 +806,15 @@ int scatter_and_plan(rw_tree_learned* L, const uint32_t* keys, uint32_t n, cudaS
   RWL_CUDA(cudaMemsetAsync(L->d_super_cursor, 0, 4 * rwt::kSupers, s));
   RWL_CUDA(cudaMemsetAsync(L->d_plan, 0, sizeof(rwt::LearnedPlan), s));
   const uint32_t tiles1 = rwt::div_up(n, rwt::kSpTile);
-  rwt::k_split<8><<<tiles1, rwt::kSpThreads, rwt::SplitCfg<8>::kSmem, s>>>(
+  rwt::launch_pdl(rwt::k_split<8>, tiles1, rwt::kSpThreads, rwt::SplitCfg<8>::kSmem, s, 
       keys, n, nullptr, 0, tiles1, 1, L->d_bounds, L->d_super_cursor, L->d_super_region, scap);
   RWL_CUDA(cudaGetLastError());
   const uint32_t tps = rwt::div_up(scap, rwt::kSpTile);
-  rwt::k_split<4><<<rwt::kSupers * tps, rwt::kSpThreads, rwt::SplitCfg<4>::kSmem, s>>>(
+  rwt::launch_pdl(rwt::k_split<4>, rwt::kSupers * tps, rwt::kSpThreads, rwt::SplitCfg<4>::kSmem, s, 
       L->d_super_region, 0, L->d_super_cursor, scap, tps, rwt::kSupers, L->d_bounds, L->d_cursor,
       L->d_region, cap);
   RWL_CUDA(cudaGetLastError());
-  rwt::k_bucket_plan<<<1, 1024, 0, s>>>(L->d_cursor, cap, L->d_super_cursor, scap, L->d_offsets,
+  rwt::launch_pdl(rwt::k_bucket_plan, 1, 1024, 0, s, L->d_cursor, cap, L->d_super_cursor, scap, L->d_offsets,
                                         L->d_order, L->d_plan);
   RWL_CUDA(cudaGetLastError());
   RWL_CUDA(cudaMemcpyAsync(L->h_plan, L->d_plan, sizeof(rwt::LearnedPlan),
@@ -946,7 +953,7 @@ int rw_tree_learned_sort(rw_tree_learned* L, const uint32_t* d_keys, uint32_t* d
     if (stats) stats->fell_back = 1;
     return rw_tree_sort_enqueue(&app, fallback_im, stream);
   }
-  rwt::k_bucket_sort<<<rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s>>>(
+  rwt::launch_pdl(rwt::k_bucket_sort, rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s, 
       L->d_region, rwt::region_cap(n), L->d_cursor, L->d_offsets, L->d_order, d_sorted);
   RWL_CUDA(cudaGetLastError());
   return RW_OK;
