@@ -2,32 +2,38 @@
 // scan, octree.
 //
 // Stage 3 replaces k_FindDups + host std::partial_sum + k_MoveDups
-// (apps/tree/cuda/03_unique.cu, cu_dispatcher.cu:597-627) with two launches:
-// per-tile ballot head counts scanned by the last block to finish, then a
+// (apps/tree/cuda/03_unique.cu, cu_dispatcher.cu:597-627) with three
+// launches: per-tile head counts, one block scanning the tile counts, then a
 // compaction of every tile at its scanned offset.
 //
-// Stage 4 is process_radix_tree_i of apps/tree/host/func_brt.hpp:45-138,
-// one thread per node.  The parent writes are made deterministic (see
-// write_node): nodes i >= 1 are the true Karras nodes and each names its
-// children once; node 0 (whose range the reference limits to [0, n_brt-1])
-// only writes the entries that sequential execution on a zeroed buffer gives.
+// Stage 4 builds the nodes of process_radix_tree_i (apps/tree/host/
+// func_brt.hpp:45-138) from nearest smaller values: the radix tree is the
+// Cartesian tree of the gap deltas, so each gap's node follows from the
+// nearest strictly smaller gap on either side (k_radix_tree; the few gaps
+// whose answer lies beyond the tile's window go to k_radix_tree_far).  Node 0
+// keeps the reference's own search over [0, n_brt-1] (brt_node, write_node);
+// nodes i >= 1 are the true Karras nodes and each names its children once, so
+// the parent writes are deterministic.
 //
 // The fused form computes stages 4 and 5 in one pass: the edge count of node i
 // needs prefix_n[parent[i]], and the parent's prefix length is the larger of
 // the two boundary deltas of i's key range (the parent splits at one end of
 // it; when that split is the global minimum the parent is the root, whose
-// prefix_n the reference computes over [0, n_brt-1]), so no second pass over
-// parent[] is needed.  Stage 6 stays a separate single-pass scan: chaining it
-// to the tree's tiles would make every tile wait for the slowest one.
+// prefix_n the reference computes over [0, n_brt-1]).
 //
-// Stage 7 follows process_oct_node (func_octree.hpp:28-112) in two kernels:
-// one writes every octree row in full (corner, cell_size, the chain child and
-// zeros elsewhere) from the radix-tree node that owns it, the next adds the
-// links from each chain's top node to its parent row with atomicMax/atomicOr.
-// Sequential ascending-i execution leaves in every child slot the largest
-// value written (node i writes only values in [off[i], off[i]+cnt[i]) and
-// these ranges grow with i), and the node mask is an OR, so the result is the
-// reference's sequential one.
+// Stage 6 run alone is a reduce, a one-block scan of the tile sums and a
+// write.  In the fused pipeline its first two steps run on the octree's tiles
+// and the octree kernel scans its own tile's counts on that prefix, writing
+// the offsets as it uses them.
+//
+// Stage 7 follows process_oct_node (func_octree.hpp:28-112) in one pass per
+// tile of nodes (k_octree): every row is written once, complete, with the
+// links whose target row lies in the tile merged in shared memory; the links
+// that leave the tile are applied afterwards with atomicMax/atomicOr
+// (k_octree_far_links).  Sequential ascending-i execution leaves in every
+// child slot the largest value written (node i writes only values in
+// [off[i], off[i]+cnt[i]) and these ranges grow with i), and the node mask is
+// an OR, so the result is the reference's sequential one.
 #include <algorithm>
 
 #include "internal.hpp"
