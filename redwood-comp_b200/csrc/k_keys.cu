@@ -10,9 +10,11 @@
 // (cu_dispatcher.cu:82-468,528-591) with a onesweep sort designed for 148 SMs:
 // one CTA per tile (grid = number of tiles, not 16), tiles handed out by an
 // atomic ticket so that every look-back waits only on tiles already running,
-// per-warp stable ranking (ballot multi-split), the tile reordered by digit in
-// shared memory, and a per-digit decoupled look-back.  Digit width is 8 or 11
-// bits; 32-bit keys take 4 or 3 passes, 64-bit keys 8 or 6.
+// per-warp stable ranking (shared-memory atomic-OR peer masks by default;
+// ballot multi-split and match.any in the variant menu), the tile reordered by
+// digit in shared memory, and a per-digit decoupled look-back.  Digit width is
+// 8 or 11 bits; 32-bit keys take 4 or 3 passes, 64-bit keys 8 or 6.  The
+// default 32-bit variant (384 threads x 24 keys) runs three blocks per SM.
 #include <algorithm>
 
 #include "internal.hpp"
