@@ -1,0 +1,62 @@
+"""bench.py's CPU-side contract: the reference arm's JSON line, and the child
+process that times the reference's own CPU pipeline (which must not take the
+bench down when that pipeline crashes on a cloud)."""
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import types
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BENCH = os.path.join(ROOT, "bench.py")
+
+
+def load_bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", BENCH)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def args(**kw):
+    base = dict(n=20000, dist="uniform", key_bits=32, seed=20260101, steps=2, warmup=1,
+                gpus=1, ref_threads=0, ref_iters=1)
+    base.update(kw)
+    return types.SimpleNamespace(**base)
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` prints one JSON line with the fields the
+    driver reads (value, unit, cpu_baseline, e2e with zero copy bytes)."""
+    r = subprocess.run([sys.executable, BENCH, "--impl", "reference", "--n", "20000",
+                        "--steps", "2", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["value"] > 0 and line["unit"] == "points/s" and line["higher_is_better"]
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_timed_in_a_child():
+    bench = load_bench()
+    from oracle import ref_available
+    if not ref_available():
+        pytest.skip("the reference's CPU library is not built here")
+    ms, cores = bench.ref_time_isolated(args(), 20260101, 2)
+    assert ms is not None, cores
+    assert len(ms) == 2 and all(t > 0 for t in ms) and cores >= 1
+
+
+def test_reference_child_failure_is_reported(monkeypatch):
+    """A child that dies (here: an interpreter that exits with an error) gives
+    (None, reason) instead of an exception."""
+    bench = load_bench()
+    monkeypatch.setattr(bench.sys, "executable", "/bin/false")
+    ms, why = bench.ref_time_isolated(args(), 20260101, 1)
+    assert ms is None and "exit 1" in why
