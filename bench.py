@@ -64,12 +64,38 @@ def parse_args():
 
 
 def make_points(rw, n, dist, seed):
+    """The workload's cloud from the library's generator (our arm)."""
     if dist == "appdata":
         return rw.generate_points(n, rw.GEN_APPDATA, 114514)
     if dist == "uniform":
         return rw.generate_points(n, rw.GEN_UNIFORM, seed)
     return rw.generate_points(n, rw.GEN_GAUSSIAN_MIXTURE, seed, n_components=32,
                               sigma_lo=4.0, sigma_hi=40.0)
+
+
+def make_points_checker(n, dist, seed):
+    """The same cloud without the product library (the reference arm and its
+    timing child): the counter-based kinds from the oracle's C restatement of
+    the generator, AppData's mt19937 stream from the reference's own code."""
+    from oracle import Oracle, RefTree
+    if dist == "appdata":
+        return RefTree().default_points(n)
+    if dist == "uniform":
+        return Oracle().generate_points(n, 1, seed)
+    return Oracle().generate_points(n, 2, seed, n_components=32, sigma_lo=4.0, sigma_hi=40.0)
+
+
+def sort_passes(a):
+    return -(-(30 if a.key_bits == 32 else 63) // (a.radix_bits or 8))
+
+
+def config_of(a):
+    """The `config` object of the JSON line; both arms print the same one."""
+    return {"workload": workload_name(a), "n_points": a.n, "key_bits": a.key_bits,
+            "radix_bits": a.radix_bits or 8, "sort_passes": sort_passes(a),
+            "parallelism": f"replicas x{a.gpus} (one cloud per GPU)",
+            "l2": f"inputs larger than L2 (points {16 * a.n / 1e6:.0f} MB per step)"
+                  if 16 * a.n > (126 << 20) else "inputs smaller than L2"}
 
 
 def workload_name(a):
@@ -189,9 +215,7 @@ def run_reference(a, rank):
     if rank != 0:
         return 0
     from oracle import ref_available
-    from __graft_entry__ import _load_package
-    rw = _load_package()
-    pts = make_points(rw, a.n, a.dist, a.seed)
+    pts = make_points_checker(a.n, a.dist, a.seed)
     note = None
     ms = None
     if a.key_bits == 32 and ref_available():
@@ -214,8 +238,7 @@ def run_reference(a, rank):
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"u{a.key_bits}", "data": "synthetic",
-        "config": {"workload": workload_name(a), "n_points": a.n,
-                   "l2": "inputs larger than L2 (points 16 B each)"},
+        "config": config_of(a),
         "cpu_baseline": {"value": val, "unit": "points/s", "cores": cores, "kind": kind,
                          "sample": f"{a.steps} full runs of stages 1-7 on the n={a.n} cloud, "
                                    f"median wall time"},
@@ -478,9 +501,7 @@ def ref_time_child(a):
     """Child side of ref_time_isolated: the same seeded cloud, the reference's
     verbatim stages 1-7 timed `--ref-iters` times; prints {"ms": [...]}."""
     from oracle import RefTree
-    from __graft_entry__ import _load_package
-    rw = _load_package()
-    pts = make_points(rw, a.n, a.dist, a.seed)
+    pts = make_points_checker(a.n, a.dist, a.seed)
     ref = RefTree()
     cores = a.ref_threads or ref.hardware_threads()
     ms = ref.time(pts, cores, a.ref_iters)
@@ -490,7 +511,7 @@ def ref_time_child(a):
 
 def ref_time_isolated(a, seed, iters):
     """Wall ms of `iters` runs of the reference's own CPU pipeline (oracle/_ref)
-    on the cloud make_points(n, dist, seed) gives, in a child process: the
+    on the cloud make_points_checker(n, dist, seed) gives, in a child process: the
     reference's stage 7 writes out of bounds on some clouds (negative octree
     offsets reach func_octree.hpp:101), which must not take this process down.
     Returns (ms list, cores) or (None, reason)."""
@@ -570,7 +591,7 @@ def main():
     im = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
     if a.sort_variant >= 0:
         im.set_sort_variant(a.sort_variant)
-    passes = -(-(30 if a.key_bits == 32 else 63) // (a.radix_bits or 8))
+    passes = sort_passes(a)
 
     def barrier():
         if world > 1:
@@ -742,10 +763,7 @@ def main():
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"u{a.key_bits}", "data": "synthetic",
-        "config": {"workload": workload_name(a), "n_points": a.n, "key_bits": a.key_bits,
-                   "radix_bits": a.radix_bits or 8, "sort_passes": passes,
-                   "parallelism": f"replicas x{world} (one cloud per GPU)",
-                   "l2": "inputs larger than L2 (points 268 MB per step)"},
+        "config": config_of(a),
         "n_unique": u, "n_octree_nodes": m, "mismatches_vs_oracle": mismatches,
         "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
                               "frac": round(pipe_gbs / hbm, 4)},

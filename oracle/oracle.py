@@ -172,6 +172,20 @@ class Oracle:
                             ctypes.c_float(range_))
         return keys
 
+    def generate_points(self, n: int, kind: int, seed: int, min_coord: float = 0.0,
+                        range_: float = 1024.0, n_components: int = 32,
+                        sigma_lo: float = 4.0, sigma_hi: float = 40.0) -> np.ndarray:
+        """The library's counter-based clouds (GEN_UNIFORM = 1,
+        GEN_GAUSSIAN_MIXTURE = 2) restated in C, byte for byte: [n, 4] float32."""
+        pts = np.zeros((n, 4), np.float32)
+        rc = self.lib.orc_generate_points(
+            _ptr(pts), ctypes.c_uint64(n), ctypes.c_int(kind), ctypes.c_uint64(seed),
+            ctypes.c_float(min_coord), ctypes.c_float(range_), ctypes.c_int(n_components),
+            ctypes.c_float(sigma_lo), ctypes.c_float(sigma_hi))
+        if rc:
+            raise ValueError(f"orc_generate_points: status {rc}")
+        return pts
+
     def sort(self, keys: np.ndarray) -> np.ndarray:
         keys = np.array(keys, copy=True)
         bits = 32 if keys.dtype == np.uint32 else 64

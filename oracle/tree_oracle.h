@@ -74,6 +74,12 @@ void orc_morton(const float* points, void* keys, uint32_t n, int key_bits,
 void orc_sort(void* keys, uint32_t n, int key_bits);
 uint64_t orc_fnv1a64(const void* data, size_t bytes);
 
+/* Seeded clouds identical to the library's rw_tree_generate_points for its
+ * counter-based kinds (points_oracle.c); kind 1 uniform, 2 Gaussian mixture. */
+enum { ORC_GEN_UNIFORM = 1, ORC_GEN_GAUSSIAN_MIXTURE = 2 };
+int orc_generate_points(float* out, uint64_t n, int kind, uint64_t seed, float min_coord,
+                        float range, int n_components, float sigma_lo, float sigma_hi);
+
 #ifdef __cplusplus
 }
 #endif

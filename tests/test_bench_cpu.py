@@ -60,3 +60,29 @@ def test_reference_child_failure_is_reported(monkeypatch):
     monkeypatch.setattr(bench.sys, "executable", "/bin/false")
     ms, why = bench.ref_time_isolated(args(), 20260101, 1)
     assert ms is None and "exit 1" in why
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm builds its cloud from the oracle's generators and
+    times the reference's own code: librw_tree.so is never mapped, and its
+    config object is the one our arm prints."""
+    code = (
+        "import sys, json, types; sys.argv=['bench.py'];"
+        "import importlib.util as u;"
+        f"spec=u.spec_from_file_location('b', {BENCH!r}); b=u.module_from_spec(spec);"
+        "spec.loader.exec_module(b);"
+        "a=types.SimpleNamespace(n=20000, dist='uniform', key_bits=32, radix_bits=0,"
+        " seed=20260101, steps=2, warmup=1, gpus=1, ref_threads=0, ref_iters=1);"
+        "b.run_reference(a, 0);"
+        "maps=open('/proc/self/maps').read();"
+        "print(json.dumps({'product_mapped': 'librw_tree' in maps,"
+        " 'config': b.config_of(a)}))")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    ref_line, probe = lines[0], lines[-1]
+    assert probe["product_mapped"] is False
+    assert ref_line["config"] == probe["config"]
+    assert set(probe["config"]) >= {"workload", "n_points", "key_bits", "radix_bits",
+                                    "sort_passes", "parallelism"}

@@ -147,3 +147,15 @@ def test_reference_verbatim_stage1_equals_oracle(rw):
     keys, n_unique, _ = ref.verbatim(pts, 4)
     assert np.array_equal(keys, Oracle().morton(pts))
     assert n_unique == 307151
+
+
+@pytest.mark.parametrize("kind,kw", [(1, {}), (2, dict(n_components=32, sigma_lo=4.0,
+                                                        sigma_hi=40.0)),
+                                     (2, dict(n_components=9, sigma_lo=2.0, sigma_hi=20.0))])
+def test_oracle_generators_equal_the_library(rw, oracle, kind, kw):
+    """The C restatement of the counter-based generators gives the library's
+    clouds byte for byte (the reference arm of the benchmark relies on it)."""
+    for n, seed in ((1, 3), (1000, 20260101), (70001, 7)):
+        want = rw.generate_points(n, kind, seed, **kw)
+        got = oracle.generate_points(n, kind, seed, **kw)
+        assert got.tobytes() == want.tobytes(), (kind, n, seed)
