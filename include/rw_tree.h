@@ -299,6 +299,20 @@ int rw_tree_sort_profile(rw_tree_app_data* app, rw_tree_im_storage* im, rw_strea
                          int32_t reps, float* kernel_ms, int32_t max_kernels,
                          int32_t* n_kernels);
 
+/* Test hook of the sort's bounded wait.  The reference's look-back spins
+ * without a bound (an unsigned `k >= 0` loop, cu_dispatcher.cu:376) and its
+ * only error path is CUDA_CHECK (redwood/cuda/helpers.cuh:12-20); here every
+ * wait gives up after a number of polls and reports RW_ERR_TIMEOUT.  This
+ * call makes that happen on purpose, without any fault: it builds the digit
+ * histograms of app->u_morton_keys, then runs the first onesweep pass into
+ * app->u_morton_keys_alt with its first tile left out, so that every other
+ * tile waits on a descriptor nothing publishes and gives up after spin_limit
+ * polls.  Every write stays inside u_morton_keys_alt[0, n).  Needs at least
+ * two tiles of keys; returns RW_ERR_TIMEOUT, and the scratch is fit for the
+ * next normal run. */
+int rw_tree_sort_lookback_probe(rw_tree_app_data* app, rw_tree_im_storage* im,
+                                uint32_t spin_limit, rw_stream_t stream);
+
 /* ---- learned-CDF bucketed sort (32-bit keys) -------------------------------
  * No reference counterpart.  A 64K-key stratified sample is sorted and 4,095
  * bucket boundaries are placed, one per 16 sample ranks: at the sample key of
@@ -382,7 +396,9 @@ int rw_tree_mlp_forward(const float* params, const float* x, uint32_t rows, floa
  * the driver's allocation locks, a plugin given only pointers and a stream).
  * No counterpart in the reference.  Same result as rw_tree_run_stage3: the
  * unique keys of sorted_keys[0, n) go to unique_keys and their count to
- * *n_unique (host memory); synchronous on `stream`.  Its scratch is a fixed
+ * *n_unique (host memory); synchronous on `stream`.  Both key buffers must be
+ * 16-byte aligned and must not overlap (RW_ERR_ARG otherwise: every tile
+ * writes its output while other tiles still read the input).  Its scratch is a fixed
  * array inside the library (about 64 KiB on every GPU that loads it), so it
  * never allocates; n above RW_NOALLOC_MAX_KEYS is rejected with RW_ERR_ARG.
  * The first call on each device looks the array's address up (make that call

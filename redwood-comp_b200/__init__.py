@@ -102,7 +102,7 @@ EXPORTS = (
     "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
     "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
-    "rw_tree_sort_profile",
+    "rw_tree_sort_profile", "rw_tree_sort_lookback_probe",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
     "rw_tree_learned_set_group", "rw_tree_im_storage_set_learned",
     "rw_tree_im_storage_learned_stats", "rw_tree_host_submit", "rw_tree_host_collect",
@@ -358,6 +358,15 @@ def sort_keys(keys, out, im: ImStorage, stream=None) -> None:
     c.u_morton_keys, c.u_morton_keys_alt = keys.data_ptr(), out.data_ptr()
     _check(lib().rw_tree_sort_enqueue(ctypes.byref(c), im.handle, _stream_handle(stream)),
            "sort_enqueue")
+
+
+def sort_lookback_probe(app: AppData, im: ImStorage, spin_limit: int, stream=None) -> int:
+    """Runs the sort's first pass with its first tile left out, so that every
+    other tile's bounded look-back wait runs out (rw_tree_sort_lookback_probe);
+    returns the rw_status code (RW_ERR_TIMEOUT when the bound works)."""
+    return int(lib().rw_tree_sort_lookback_probe(ctypes.byref(app.c), im.handle,
+                                                 ctypes.c_uint32(spin_limit),
+                                                 _stream_handle(stream)))
 
 
 def profile_sort(keys, out, im: ImStorage, reps: int = 5, stream=None) -> dict:

@@ -362,6 +362,19 @@ int rw_tree_sort_profile(rw_tree_app_data* app, rw_tree_im_storage* im, rw_strea
   return rc;
 }
 
+int rw_tree_sort_lookback_probe(rw_tree_app_data* app, rw_tree_im_storage* im,
+                                uint32_t spin_limit, rw_stream_t stream) {
+  if (int rc = check(app, im, kKeys | kAlt)) return rc;
+  if (spin_limit == 0) return RW_ERR_ARG;
+  if (rwt::div_up(app->n_input, rwt::sort_variant_tile(im->sort_variant)) < 2)
+    return RW_ERR_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (int rc = clear_all(im, s)) return rc;
+  RW_CUDA(rwt::launch_sort_lookback_probe(bufs_of(*app, im), scratch_of(im), plan_of(*app, im),
+                                          spin_limit, s));
+  return sync_status(im, s);
+}
+
 // ---- stage 3: unique (cu_dispatcher.cu:597-627) -------------------------------
 int rw_tree_run_stage3(rw_tree_app_data* app, rw_tree_im_storage* im,
                        rw_stream_t stream) {

@@ -176,44 +176,4 @@ __device__ __forceinline__ uint32_t tile_segment(const SegTable& s, const TileMa
   return lo;
 }
 
-// Warp-cooperative look-back for a single-value chained scan.  Called by one
-// whole warp of the tile `tile` (> first).  desc[t] holds tile t's descriptor;
-// the chain starts at tile `first` (the segment's first tile).  Returns the
-// exclusive prefix of `tile` within its segment.  On a timeout it reports the
-// error and returns 0.
-__device__ __forceinline__ uint32_t warp_lookback(const uint32_t* desc,
-                                                  uint32_t tile,
-                                                  DevStatus* st,
-                                                  uint32_t site,
-                                                  uint32_t first = 0) {
-  const uint32_t lane = lane_id();
-  uint32_t excl = 0;
-  int64_t hi = (int64_t)tile - 1;  // nearest predecessor still to read
-  uint32_t spin = 0;
-  while (true) {
-    const int64_t idx = hi - (int64_t)lane;
-    const uint32_t d = idx >= (int64_t)first ? ld_relaxed(desc + idx) : (kFlagInc);
-    const uint32_t f = d & kFlagMask;
-    const uint32_t inc_mask = __ballot_sync(0xffffffffu, f == kFlagInc);
-    const uint32_t bad_mask = __ballot_sync(0xffffffffu, f == 0u);
-    // lanes up to and including the first inclusive descriptor count
-    const uint32_t first_inc = inc_mask ? (uint32_t)(__ffs(inc_mask) - 1) : 32u;
-    const uint32_t need = first_inc == 32u ? 0xffffffffu
-                                           : (first_inc == 31u ? 0xffffffffu
-                                                               : ((2u << first_inc) - 1u));
-    if (bad_mask & need) {
-      if (++spin > kSpinLimit || device_failed(st)) {
-        if (lane == 0) report_error(st, RW_ERR_TIMEOUT, site);
-        return 0;
-      }
-      backoff(spin);
-      continue;
-    }
-    const uint32_t mine = ((need >> lane) & 1u) ? (d >> 2) : 0u;
-    excl += warp_sum(mine);
-    if (first_inc != 32u) return excl;
-    hi -= 32;
-  }
-}
-
 }  // namespace rwt

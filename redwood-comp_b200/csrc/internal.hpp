@@ -113,6 +113,8 @@ struct Scratch {
   uint32_t* scan_desc = nullptr;
   uint32_t* tile_ctr = nullptr;
   DevStatus* status = nullptr;
+  // polls of a look-back wait before it gives up with RW_ERR_TIMEOUT
+  uint32_t spin_limit = kSpinLimit;
   // tree_far_cap entries of 16 bytes: radix-tree gaps left to the far search
   // (gap, segment: 8 bytes each), then the octree's far links (16 bytes each)
   uint32_t* tree_far = nullptr;
@@ -151,12 +153,18 @@ cudaError_t launch_keys(const Bufs& b, const Scratch& sc, const Plan& pl, bool e
 // kernel and one after each pass (profiling only).
 cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,
                                cudaStream_t s, cudaEvent_t* marks = nullptr);
+// Test hook of the bounded look-back wait: the digit histograms of b.keys,
+// then pass 0 of the sort into b.alt with tile 0 left out, so that every
+// other tile's look-back waits on a row nothing publishes and gives up after
+// spin_limit polls (RW_ERR_TIMEOUT in the status word).  Needs >= 2 tiles.
+cudaError_t launch_sort_lookback_probe(const Bufs& b, const Scratch& sc, const Plan& pl,
+                                       uint32_t spin_limit, cudaStream_t s);
 cudaError_t launch_unique(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
-// The unique kernel on caller-given scratch: `desc` holds one word per
-// kUniqueTile keys and, like *tile_ctr and *status, must be zero.
+// The unique kernels on caller-given scratch: `counts` holds one word per
+// kUniqueTile keys plus one and, like *status, must be zero.
 cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
-                              uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
-                              int num_sms, cudaStream_t s);
+                              uint32_t* counts, DevStatus* status, int num_sms,
+                              cudaStream_t s);
 // Stage 4 alone (edges = false) or stages 4 and 5 in one pass (edges = true).
 cudaError_t launch_radix_tree(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
                               cudaStream_t s);

@@ -177,7 +177,8 @@ template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
-              uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st) {
+              uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st,
+              uint32_t spin_limit) {
   pdl_enter();
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
   constexpr int RADIX = C::RADIX, NW = C::NW, TILE = C::TILE;
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
         spin = 0;
         continue;
       }
-      if (++spin > kSpinLimit || device_failed(st)) {
+      if (++spin > spin_limit || device_failed(st)) {
         report_error(st, RW_ERR_TIMEOUT, kSiteSort);
         break;
       }
@@ -349,9 +350,10 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
   return cudaGetLastError();
 }
 
+// probe_spins != 0: the bounded-wait test hook (launch_sort_lookback_probe).
 template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
-                     cudaEvent_t* marks) {
+                     cudaEvent_t* marks, uint32_t probe_spins) {
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
   auto kern = k_binning<K, D, THREADS, KPT, RANK, MINB>;
   const uint32_t tiles = pl.sort_map.n_tiles;
@@ -366,6 +368,18 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   K* keys = static_cast<K*>(b.keys);
   K* alt = static_cast<K*>(b.alt);
   K* tmp = static_cast<K*>(b.tmp);
+  if (probe_spins) {
+    // pass 0 with the tile ticket starting at 1: tile 0 never runs, so its
+    // descriptor row stays unpublished and every other tile's look-back runs
+    // into its spin limit; tiles 1 .. tiles-1 are launched (all in range)
+    if (tiles < 2 || pl.seg.count != 1) return cudaErrorInvalidValue;
+    e = cudaMemsetAsync(sc.tile_ctr + kCtrSortBase, 0x01, 1, s);
+    if (e != cudaSuccess) return e;
+    launch_pdl(kern, tiles - 1, THREADS, C::kSmem, s, static_cast<const K*>(keys), alt, pl.seg,
+               pl.sort_map, 0, sc.sort_desc, sc.tile_ctr + kCtrSortBase, sc.status,
+               probe_spins);
+    return cudaGetLastError();
+  }
   const K* src = keys;
   for (int p = 0; p < sc.passes; ++p) {
     K* dst = ((sc.passes - 1 - p) % 2 == 0) ? alt : tmp;
@@ -373,7 +387,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
       launch_pdl(kern, tiles, THREADS, C::kSmem, s, 
           src, dst, pl.seg, pl.sort_map, p * D,
           sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
-          sc.tile_ctr + kCtrSortBase + p, sc.status);
+          sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (marks) cudaEventRecord(marks[1 + p], s);
@@ -383,7 +397,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
 }
 
 using PassFn = cudaError_t (*)(const Bufs&, const Scratch&, const Plan&, cudaStream_t,
-                               cudaEvent_t*);
+                               cudaEvent_t*, uint32_t);
 
 struct SortVariant {
   int key_bits, radix_bits, threads, kpt, rank;
@@ -476,7 +490,18 @@ cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,
   if (v < 0 || v >= kNumVariants || kVariants[v].key_bits != b.key_bits ||
       kVariants[v].radix_bits != sc.radix_bits)
     return cudaErrorInvalidValue;
-  return kVariants[v].fn(b, sc, pl, s, marks);
+  return kVariants[v].fn(b, sc, pl, s, marks, 0u);
+}
+
+cudaError_t launch_sort_lookback_probe(const Bufs& b, const Scratch& sc, const Plan& pl,
+                                       uint32_t spin_limit, cudaStream_t s) {
+  const int v = sc.sort_variant;
+  if (v < 0 || v >= kNumVariants || kVariants[v].key_bits != b.key_bits ||
+      kVariants[v].radix_bits != sc.radix_bits || spin_limit == 0)
+    return cudaErrorInvalidValue;
+  cudaError_t e = launch_keys(b, sc, pl, false, true, s);
+  if (e != cudaSuccess) return e;
+  return kVariants[v].fn(b, sc, pl, s, nullptr, spin_limit);
 }
 
 }  // namespace rwt

@@ -1419,16 +1419,15 @@ cudaError_t launch_unique(const Bufs& b, const Scratch& sc, const Plan& pl, cuda
 }
 
 cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,
-                              uint32_t* desc, uint32_t* tile_ctr, DevStatus* status,
-                              int num_sms, cudaStream_t s) {
+                              uint32_t* counts, DevStatus* status, int num_sms,
+                              cudaStream_t s) {
   Bufs b;
   b.key_bits = key_bits;
   b.alt = const_cast<void*>(sorted);
   b.keys = out;
   Scratch sc;
   sc.num_sms = num_sms;
-  sc.unique_desc = desc;
-  sc.tile_ctr = tile_ctr - kCtrUnique;
+  sc.unique_desc = counts;
   sc.status = status;
   const Plan pl = single_plan(n, 0, status, 0);
   return launch_unique(b, sc, pl, s);

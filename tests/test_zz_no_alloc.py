@@ -54,8 +54,8 @@ def via_noalloc(rw, keys, key_bits):
 
 @pytest.mark.parametrize("key_bits", [32, 64])
 def test_noalloc_unique_equals_stage3_two_calls_in_a_row(rw, key_bits):
-    # a large call then a smaller one: the second finds the first one's
-    # look-back words in the shared scratch and must not be misled by them
+    # a large call then a smaller one, back to back on the one scratch array
+    # inside the library: each must give exactly what stage 3 gives
     for n, seed in ((1_000_003, 11), (77_777, 12)):
         keys = sorted_keys_with_runs(n, seed, key_bits)
         want_u, want = via_stage3(rw, keys, key_bits)
@@ -74,3 +74,24 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(rw):
     rc = rw.lib().rw_tree_unique_noalloc(dummy, dummy, ctypes.c_uint32(0),
                                          ctypes.c_int32(32), ctypes.byref(count), None)
     assert rc == rw.RW_ERR_ARG
+
+
+def test_noalloc_rejects_unaligned_or_overlapping_buffers(rw):
+    """Host-side argument checks: the addresses below are never dereferenced,
+    because both checks come before any device access."""
+    count = ctypes.c_uint32(0)
+    a, b = ctypes.c_void_p(1 << 20), ctypes.c_void_p(1 << 21)
+    odd = ctypes.c_void_p((1 << 20) + 4)
+    for key_bits in (32, 64):
+        assert rw.lib().rw_tree_unique_noalloc(odd, b, ctypes.c_uint32(100),
+                                               ctypes.c_int32(key_bits), ctypes.byref(count),
+                                               None) == rw.RW_ERR_ARG
+        assert rw.lib().rw_tree_unique_noalloc(a, odd, ctypes.c_uint32(100),
+                                               ctypes.c_int32(key_bits), ctypes.byref(count),
+                                               None) == rw.RW_ERR_ARG
+    # in place, and overlapping by one key
+    assert rw.lib().rw_tree_unique_noalloc(a, a, ctypes.c_uint32(100), ctypes.c_int32(32),
+                                           ctypes.byref(count), None) == rw.RW_ERR_ARG
+    near = ctypes.c_void_p((1 << 20) + 16 * 24)
+    assert rw.lib().rw_tree_unique_noalloc(a, near, ctypes.c_uint32(100), ctypes.c_int32(32),
+                                           ctypes.byref(count), None) == rw.RW_ERR_ARG
