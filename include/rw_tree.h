@@ -13,6 +13,8 @@
  *
  * Buffer contract (app_data.hpp:139-157): stage 2 leaves the sorted keys in
  * u_morton_keys_alt, stage 3 leaves the unique keys in u_morton_keys.
+ * Every output is bit-exact with the reference's functions unless an option
+ * of rw_tree_im_storage_set_options says otherwise.
  *
  * Errors: every call returns RW_OK (0) or an rw_status code; the C++ layer in
  * redwood_tree/ turns a non-zero code into std::runtime_error as the
@@ -111,6 +113,27 @@ int rw_tree_sort_variant_info(int32_t idx, int32_t* key_bits, int32_t* radix_bit
                               int32_t* rank_mode);
 /* Selects variant idx (its key and digit width must match the storage). */
 int rw_tree_im_storage_set_sort_variant(rw_tree_im_storage* im, int32_t idx);
+/* Options that change the reference's outputs on purpose, both off by
+ * default (0 keeps every output bit-exact with the reference):
+ *   RW_TREE_OPT_GEOMETRIC_DELTA - the radix tree's delta is clz(a ^ b) - 2
+ *     for 32-bit keys, the true common-prefix length of 30-bit codes, so that
+ *     octree levels and child links are geometrically exact.  The reference's
+ *     delta_u32 is clz - 1 (func_brt.hpp:27-33), written for 31-bit codes.
+ *     64-bit codes are 63 bits wide and their clz - 1 is already exact, so
+ *     the option changes nothing for them.
+ *   RW_TREE_OPT_LINK_LEAVES - after the octree, the reference's leaf linker
+ *     process_link_leaf (func_octree.hpp:114-163; k_LinkLeafNodes,
+ *     07_octree.cu:228-258, whose launch cu_dispatcher.cu:738-749 leaves
+ *     commented out) for every radix-tree node, with the result of running
+ *     them in ascending order: each leaf index goes into its slot of the
+ *     bottom octree row of the nearest ancestor that owns rows, and the
+ *     slot's child_leaf_mask bit is cleared (set_leaf, func_octree.hpp:18-25).
+ *     The walk up the tree stops after 31 steps (the reference's CPU walk has
+ *     no bound and never ends at a root without rows).
+ * Applies to the stage calls and the fused pipeline of this scratch. */
+#define RW_TREE_OPT_GEOMETRIC_DELTA 1
+#define RW_TREE_OPT_LINK_LEAVES 2
+int rw_tree_im_storage_set_options(rw_tree_im_storage* im, int32_t options);
 /* ~ImStorage (im_storage.cu:42-52). */
 int rw_tree_im_storage_destroy(rw_tree_im_storage* im);
 /* ImStorage::clearSmem (im_storage.cu:53-60): zeroes histograms, descriptors

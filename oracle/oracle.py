@@ -62,7 +62,12 @@ class _OrcTree(ctypes.Structure):
         ("n_unique", ctypes.c_uint32),
         ("n_brt_nodes", ctypes.c_uint32),
         ("n_octree_nodes", ctypes.c_uint32),
+        ("options", ctypes.c_int),
     ]
+
+
+# Options outside the bit-exact contract with the reference (tree_oracle.h).
+OPT_GEOMETRIC_DELTA, OPT_LINK_LEAVES = 1, 2
 
 
 @dataclass
@@ -194,8 +199,9 @@ class Oracle:
 
     def run(self, points: np.ndarray, key_bits: int = 32,
             min_coord: float = 0.0, range_: float = 1024.0,
-            capacity: int | None = None) -> TreeResult:
-        """Stages 1-7 on `points` ([n,4] float32).  status != 0 stops early."""
+            capacity: int | None = None, options: int = 0) -> TreeResult:
+        """Stages 1-7 on `points` ([n,4] float32).  status != 0 stops early.
+        `options`: OPT_* bits (0: the reference's own behaviour)."""
         points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
         n = points.shape[0]
         cap = octree_capacity(n) if capacity is None else capacity
@@ -211,7 +217,7 @@ class Oracle:
             children=_ptr(r.children).value, corner=_ptr(r.corner).value,
             cell_size=_ptr(r.cell_size).value,
             child_node_mask=_ptr(r.child_node_mask).value,
-            child_leaf_mask=_ptr(r.child_leaf_mask).value)
+            child_leaf_mask=_ptr(r.child_leaf_mask).value, options=options)
         tp = ctypes.byref(t)
         status = self.lib.orc_stage1(tp)
         if status == 0:
@@ -283,7 +289,11 @@ class RefTree:
             raise RuntimeError(f"ref_cpu_time failed: {rc}")
         return ms
 
-    def canonical(self, points: np.ndarray, n_threads: int = 1) -> TreeResult:
+    def canonical(self, points: np.ndarray, n_threads: int = 1,
+                  link_leaves: bool = False) -> TreeResult:
+        """The reference's own per-element functions in the canonical dataflow;
+        with link_leaves, its process_link_leaf after stage 7 (status 4 when
+        some leaf's walk up the tree would never end on this cloud)."""
         points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
         n = points.shape[0]
         cap = int(self.lib.ref_octree_capacity(ctypes.c_uint32(n)))
@@ -300,8 +310,8 @@ class RefTree:
             cell_size=_ptr(r.cell_size).value,
             child_node_mask=_ptr(r.child_node_mask).value,
             child_leaf_mask=_ptr(r.child_leaf_mask).value)
-        rc = self.lib.ref_canonical(_ptr(points), ctypes.c_uint32(n),
-                                    ctypes.c_int(n_threads), ctypes.byref(o))
+        fn = self.lib.ref_canonical_linked if link_leaves else self.lib.ref_canonical
+        rc = fn(_ptr(points), ctypes.c_uint32(n), ctypes.c_int(n_threads), ctypes.byref(o))
         r.status = int(rc)
         r.n_unique, r.n_brt_nodes = o.n_unique, o.n_brt_nodes
         r.n_octree_nodes = o.n_octree_nodes

@@ -128,8 +128,29 @@ int ref_cpu_time(const float* pts, uint32_t n, int n_threads, int iters,
 // success, 2 when fewer than 3 distinct keys exist (the reference's root range
 // [0, n_brt-1] is empty below that), 3 when the octree overflows AppData's
 // capacity.
+static int canonical_impl(const float* pts, uint32_t n, int n_threads,
+                          ref_canonical_out* out, bool link_leaves);
+
 int ref_canonical(const float* pts, uint32_t n, int n_threads,
                   ref_canonical_out* out) {
+  return canonical_impl(pts, n, n_threads, out, false);
+}
+
+// The same, then the reference's own leaf linker process_link_leaf
+// (func_octree.hpp:114-163) for every radix-tree node in ascending order - the
+// k_LinkLeafNodes launch the reference leaves commented out
+// (cu_dispatcher.cu:738-749).  Its walk up the radix tree has no bound and
+// never ends once it reaches the root without octree nodes (the root is its
+// own parent); a cloud where some walk would get there returns 4 before any
+// call, so that only clouds on which the reference's function is total are
+// compared.
+int ref_canonical_linked(const float* pts, uint32_t n, int n_threads,
+                         ref_canonical_out* out) {
+  return canonical_impl(pts, n, n_threads, out, true);
+}
+
+static int canonical_impl(const float* pts, uint32_t n, int n_threads,
+                          ref_canonical_out* out, bool link_leaves) {
   if (n < 1 || n_threads < 1) return 1;
   AppData app(std::pmr::new_delete_resource(), n);
   load_points(app, pts);
@@ -213,6 +234,27 @@ int ref_canonical(const float* pts, uint32_t n, int n_threads,
         app.u_edge_count.data(), app.get_unique_morton_keys(),
         app.brt.u_prefix_n.data(), app.brt.u_parents.data(), app.min_coord,
         app.range);
+  }
+  if (link_leaves) {
+    for (int i = 0; i < n_brt; ++i) {
+      if (!app.brt.u_has_leaf_left[i] && !app.brt.u_has_leaf_right[i]) continue;
+      int rt = i, steps = 0;
+      while (app.u_edge_count[rt] == 0 && steps <= 64) {
+        rt = app.brt.u_parents[rt];
+        ++steps;
+      }
+      if (app.u_edge_count[rt] == 0) return 4;
+    }
+    for (int i = 0; i < n_brt; ++i) {
+      cpu::kernels::process_link_leaf(
+          i, reinterpret_cast<int(*)[8]>(app.oct.u_children.data()),
+          app.oct.u_child_leaf_mask.data(), app.u_edge_offset.data(),
+          app.u_edge_count.data(), app.get_unique_morton_keys(),
+          reinterpret_cast<const bool*>(app.brt.u_has_leaf_left.data()),
+          reinterpret_cast<const bool*>(app.brt.u_has_leaf_right.data()),
+          app.brt.u_prefix_n.data(), app.brt.u_parents.data(),
+          app.brt.u_left_child.data());
+    }
   }
 
   std::memcpy(out->prefix_n, app.brt.u_prefix_n.data(), size_t(n));

@@ -174,9 +174,13 @@ int orc_stage3(orc_tree* t) {
 /* ------------------------------------------------------------------------ */
 
 /* delta = clz(a ^ b) - 1 over the key word (func_brt.hpp:27-33), kept with
- * its -1 even though 32-bit codes have two leading zero bits. */
+ * its -1 even though 32-bit codes have two leading zero bits; with
+ * ORC_OPT_GEOMETRIC_DELTA, 32-bit keys subtract one more (g_delta_bias). */
+static int g_delta_bias = 0;
+
 static inline int delta(uint64_t a, uint64_t b, int key_bits) {
-  if (key_bits == 32) return (uint8_t)(__builtin_clz((uint32_t)(a ^ b)) - 1);
+  if (key_bits == 32)
+    return (uint8_t)(__builtin_clz((uint32_t)(a ^ b)) - 1 - g_delta_bias);
   return (uint8_t)(__builtin_clzll(a ^ b) - 1);
 }
 
@@ -253,9 +257,11 @@ int orc_stage4(orc_tree* t) {
   memset(t->has_leaf_right, 0, (size_t)n);
   memset(t->left_child, 0, 4 * (size_t)n);
   memset(t->parents, 0, 4 * (size_t)n);
+  g_delta_bias = (t->options & ORC_OPT_GEOMETRIC_DELTA) && t->key_bits == 32 ? 1 : 0;
   for (int i = 0; i < n; ++i)
     brt_node(i, n, t->keys, t->key_bits, t->prefix_n, t->has_leaf_left,
              t->has_leaf_right, t->left_child, t->parents);
+  g_delta_bias = 0;
   return ORC_OK;
 }
 
@@ -350,6 +356,50 @@ int orc_stage7(orc_tree* t) {
       t->cell_size[oct] = t->range / (float)(1 << (top - root_level));
     }
   }
+  if (t->options & ORC_OPT_LINK_LEAVES) return orc_link_leaves(t);
+  return ORC_OK;
+}
+
+/* process_link_leaf (func_octree.hpp:114-163) for node i: each leaf child of
+ * i goes into slot (leaf's code at level prefix_n[i]/3 + 1) & 7 of the bottom
+ * octree node of the nearest radix-tree ancestor-or-self that owns octree
+ * nodes; set_leaf (func_octree.hpp:18-25) clears that slot's leaf-mask bit.
+ * Two definitions where the reference's are not total:
+ *   - the walk up the radix tree stops after 31 steps, as the left-leaf walk
+ *     of the CUDA restatement does (07_octree.cu:136-147); the CPU version's
+ *     walk never ends when it reaches the root with no octree nodes (the
+ *     root's parent is itself);
+ *   - the level shift B - 3 * level is negative for 32-bit keys when
+ *     prefix_n[i] = 30 (possible only with the reference's clz - 1); the
+ *     shift count is then taken modulo 32, as the x86 shift instruction a
+ *     g++ build of the reference executes does. */
+static void link_leaf(orc_tree* t, int i) {
+  const int kb = t->key_bits;
+  const int B = code_bits(kb);
+  const int W = kb == 32 ? 32 : 64;
+  for (int side = 0; side < 2; ++side) {
+    const uint8_t has = side ? t->has_leaf_right[i] : t->has_leaf_left[i];
+    if (!has) continue;
+    const int leaf = t->left_child[i] + side;
+    const int level = t->prefix_n[i] / 3 + 1;
+    const int sh = (B - 3 * level) & (W - 1);
+    const uint64_t pre = kget(t->keys, kb, (size_t)leaf) >> sh;
+    const unsigned which = (unsigned)(pre & 7u);
+    int rt = i, counter = 0;
+    while (t->edge_count[rt] == 0) {
+      rt = t->parents[rt];
+      if (++counter > 30) break;
+    }
+    const int bottom = t->edge_offset[rt];
+    t->children[8 * (size_t)bottom + which] = leaf;
+    t->child_leaf_mask[bottom] &= ~(1 << which);
+  }
+}
+
+int orc_link_leaves(orc_tree* t) {
+  if (!t || t->n_unique < 3) return ORC_ERR_DEGENERATE;
+  const int n = (int)t->n_brt_nodes;
+  for (int i = 0; i < n; ++i) link_leaf(t, i);
   return ORC_OK;
 }
 

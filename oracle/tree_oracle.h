@@ -56,7 +56,20 @@ typedef struct orc_tree {
   uint32_t n_unique;
   uint32_t n_brt_nodes;
   uint32_t n_octree_nodes;
+  int options; /* ORC_OPT_* bits; 0 is the reference's own behaviour */
 } orc_tree;
+
+/* Options outside the bit-exact contract with the reference (both change its
+ * outputs on purpose):
+ *   ORC_OPT_GEOMETRIC_DELTA - delta = clz(a ^ b) - 2 for 32-bit keys, the true
+ *     common-prefix length of 30-bit codes (the reference's clz - 1 of
+ *     func_brt.hpp:27-33 counts one of the two always-zero top bits).  64-bit
+ *     codes are 63 bits wide, so their clz - 1 is already the true length and
+ *     the option changes nothing for them.
+ *   ORC_OPT_LINK_LEAVES - after stage 7, process_link_leaf
+ *     (func_octree.hpp:114-163) for every radix-tree node in ascending order,
+ *     the launch the reference leaves commented out (cu_dispatcher.cu:738-749). */
+enum { ORC_OPT_GEOMETRIC_DELTA = 1, ORC_OPT_LINK_LEAVES = 2 };
 
 uint32_t orc_capacity(uint32_t n_input);
 int orc_stage1(orc_tree* t);
@@ -67,6 +80,8 @@ int orc_stage5(orc_tree* t);
 int orc_stage6(orc_tree* t);
 int orc_stage7(orc_tree* t);
 int orc_run_all(orc_tree* t);
+/* The leaf links alone (stage 7 calls it under ORC_OPT_LINK_LEAVES). */
+int orc_link_leaves(orc_tree* t);
 
 /* Single stages on raw arrays, for tests of one kernel at a time. */
 void orc_morton(const float* points, void* keys, uint32_t n, int key_bits,

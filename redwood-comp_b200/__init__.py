@@ -38,6 +38,8 @@ STATUS_NAMES = {
     7: "RW_ERR_NO_DEVICE",
 }
 COUNT_UNSET = 0xFFFFFFFF
+# options outside the reference contract (rw_tree_im_storage_set_options)
+OPT_GEOMETRIC_DELTA, OPT_LINK_LEAVES = 1, 2
 GEN_APPDATA, GEN_UNIFORM, GEN_GAUSSIAN_MIXTURE = 0, 1, 2
 DEFAULT_SEED = 114514  # app_data.hpp:32
 
@@ -102,7 +104,7 @@ EXPORTS = (
     "rw_tree_batch_total_points", "rw_tree_batch_octree_rows", "rw_tree_batch_offsets",
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
     "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
-    "rw_tree_sort_profile", "rw_tree_sort_lookback_probe",
+    "rw_tree_sort_profile", "rw_tree_sort_lookback_probe", "rw_tree_im_storage_set_options",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
     "rw_tree_learned_set_group", "rw_tree_im_storage_set_learned",
     "rw_tree_im_storage_learned_stats", "rw_tree_host_submit", "rw_tree_host_collect",
@@ -188,6 +190,12 @@ class ImStorage:
     @property
     def handle(self) -> _vp:
         return self._h
+
+    def set_options(self, options: int) -> None:
+        """OPT_GEOMETRIC_DELTA / OPT_LINK_LEAVES bits (0: the reference's own
+        outputs); see rw_tree_im_storage_set_options."""
+        _check(lib().rw_tree_im_storage_set_options(self._h, ctypes.c_int32(options)),
+               "set_options")
 
     def set_sort_variant(self, idx: int) -> None:
         _check(lib().rw_tree_im_storage_set_sort_variant(self._h, idx), "set_sort_variant")
@@ -526,6 +534,12 @@ class Batch:
         import torch
         host = np.concatenate([np.ascontiguousarray(c, np.float32).reshape(-1, 4) for c in clouds])
         self.points.copy_(torch.from_numpy(host))
+
+    def set_options(self, options: int) -> None:
+        """OPT_GEOMETRIC_DELTA / OPT_LINK_LEAVES bits (0: the reference's own
+        outputs); see rw_tree_im_storage_set_options."""
+        _check(lib().rw_tree_im_storage_set_options(self._h, ctypes.c_int32(options)),
+               "set_options")
 
     def set_sort_variant(self, idx: int) -> None:
         _check(lib().rw_tree_batch_set_sort_variant(self._h, idx), "batch_set_sort_variant")

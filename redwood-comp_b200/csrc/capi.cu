@@ -127,6 +127,10 @@ int upload_counts(const rw_tree_app_data* app, rw_tree_im_storage* im, cudaStrea
   return RW_OK;
 }
 
+bool geometric_delta(const rw_tree_im_storage* im) {
+  return (im->options & RW_TREE_OPT_GEOMETRIC_DELTA) && im->key_bits == 32;
+}
+
 int clear_all(rw_tree_im_storage* im, cudaStream_t s) {
   RW_CUDA(cudaMemsetAsync(im->d_zero, 0, im->zero_bytes, s));
   return RW_OK;
@@ -265,6 +269,13 @@ int rw_tree_im_storage_set_sort_variant(rw_tree_im_storage* im, int32_t idx) {
   return RW_OK;
 }
 
+int rw_tree_im_storage_set_options(rw_tree_im_storage* im, int32_t options) {
+  if (!im || (options & ~(RW_TREE_OPT_GEOMETRIC_DELTA | RW_TREE_OPT_LINK_LEAVES)))
+    return RW_ERR_ARG;
+  im->options = options;
+  return RW_OK;
+}
+
 int rw_tree_im_storage_destroy(rw_tree_im_storage* im) {
   if (!im) return RW_OK;
   if (im->d_zero) cudaFree(im->d_zero);
@@ -398,6 +409,8 @@ int rw_tree_run_stage4(rw_tree_app_data* app, rw_tree_im_storage* im,
   if (int rc = upload_counts(app, im, s)) return rc;
   RW_CUDA(rwt::launch_radix_tree(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), false,
                                  s));
+  if (geometric_delta(im))
+    RW_CUDA(rwt::launch_prefix_shift(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
   return sync_status(im, s);
 }
 
@@ -439,6 +452,8 @@ int rw_tree_run_stage7(rw_tree_app_data* app, rw_tree_im_storage* im,
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (int rc = upload_counts(app, im, s)) return rc;
   RW_CUDA(rwt::launch_octree(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
+  if (im->options & RW_TREE_OPT_LINK_LEAVES)
+    RW_CUDA(rwt::launch_leaf_links(bufs_of(*app, im), scratch_of(im), plan_of(*app, im), s));
   return sync_status(im, s);
 }
 
@@ -478,12 +493,21 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
   }
   RW_CUDA(rwt::launch_unique(b, sc, pl, s));
   RW_CUDA(mark());
-  RW_CUDA(rwt::launch_radix_tree(b, sc, pl, true, s));
+  if (geometric_delta(im)) {
+    // the tree with the reference's delta, every prefix lowered by one, then
+    // the edge counts from the lowered prefixes
+    RW_CUDA(rwt::launch_radix_tree(b, sc, pl, false, s));
+    RW_CUDA(rwt::launch_prefix_shift(b, sc, pl, s));
+    RW_CUDA(rwt::launch_edge_count(b, sc, pl, s));
+  } else {
+    RW_CUDA(rwt::launch_radix_tree(b, sc, pl, true, s));
+  }
   RW_CUDA(mark());
   RW_CUDA(rwt::launch_edge_sums(b, sc, pl, s));
   RW_CUDA(mark());
   RW_CUDA(rwt::launch_octree(b, sc, pl, s, ev ? ev + k : nullptr, true));
   if (ev) k += 2;
+  if (im->options & RW_TREE_OPT_LINK_LEAVES) RW_CUDA(rwt::launch_leaf_links(b, sc, pl, s));
   RW_CUDA(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(rwt::DevStatus),
                           cudaMemcpyDeviceToHost, s));
   if (n_ev) *n_ev = k;

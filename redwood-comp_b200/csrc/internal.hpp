@@ -46,6 +46,9 @@ struct rw_tree_im_storage {
   rw_tree_learned* learned = nullptr;
   int32_t learned_mode = 0;
   rw_tree_learned_stats learned_stats{};
+
+  // RW_TREE_OPT_* bits (0: the reference's own behaviour)
+  int32_t options = 0;
 };
 
 namespace rwt {
@@ -177,6 +180,14 @@ cudaError_t launch_edge_scan(const Bufs& b, const Scratch& sc, const Plan& pl, c
 cudaError_t launch_edge_sums(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s);
 cudaError_t launch_octree(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
                           cudaEvent_t* marks = nullptr, bool fused_offsets = false);
+
+// Options outside the reference contract (RW_TREE_OPT_*), single cloud only:
+// prefix_n[0, n_brt) -= 1 after stage 4 (the clz - 2 delta of 32-bit keys),
+// and the leaf links after stage 7.
+cudaError_t launch_prefix_shift(const Bufs& b, const Scratch& sc, const Plan& pl,
+                                cudaStream_t s);
+cudaError_t launch_leaf_links(const Bufs& b, const Scratch& sc, const Plan& pl,
+                              cudaStream_t s);
 
 // Text returned by rw_tree_last_error (this thread).
 void set_last_error(const std::string& msg);

@@ -1326,6 +1326,111 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// options outside the reference contract (rw_tree_im_storage_set_options)
+// ---------------------------------------------------------------------------
+
+// RW_TREE_OPT_GEOMETRIC_DELTA, 32-bit keys: prefix_n[i] -= 1.  The tree's
+// shape depends only on comparisons between deltas, so building it with the
+// reference's clz - 1 and lowering every prefix by one gives exactly the tree
+// of the clz - 2 delta (every node of distinct 30-bit keys has prefix >= 1).
+__global__ void __launch_bounds__(256)
+    k_prefix_shift(uint8_t* __restrict__ prefix_n, const uint32_t* __restrict__ n_unique) {
+  pdl_enter();
+  const uint32_t nu = *n_unique;
+  if (nu < 3 || nu == RW_COUNT_UNSET) return;
+  const uint32_t n = nu - 1;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    prefix_n[i] = uint8_t(prefix_n[i] - 1u);
+}
+
+// RW_TREE_OPT_LINK_LEAVES: process_link_leaf (func_octree.hpp:114-163) for
+// every radix-tree node, as if run in ascending order after stage 7.  Leaf
+// `side` of node i goes to slot (leaf code at level prefix_n[i]/3 + 1) & 7 of
+// the bottom octree row of the nearest ancestor-or-self with octree rows.
+// The walk stops after 31 steps (the reference CPU walk has no bound and
+// never ends at a root without rows; its CUDA left-leaf walk stops there),
+// and a negative level shift (32-bit keys, prefix_n = 30) is taken modulo
+// the word width, as an x86 build of the reference does.  Returns false when
+// the node has no such leaf or the row is out of range.
+template <typename K>
+__device__ __forceinline__ bool leaf_target(int i, int side, int n, const K* __restrict__ codes,
+                                            const uint8_t* __restrict__ pn,
+                                            const uint8_t* __restrict__ hl,
+                                            const uint8_t* __restrict__ hr,
+                                            const int32_t* __restrict__ lc,
+                                            const int32_t* __restrict__ par,
+                                            const int32_t* __restrict__ ec,
+                                            const int32_t* __restrict__ off, uint32_t rows,
+                                            uint32_t* slot, int* leaf) {
+  if (!(side ? hr[i] : hl[i])) return false;
+  constexpr int B = KeyTraits<K>::kCodeBits, W = KeyTraits<K>::kWordBits;
+  const int lf = min(max(lc[i] + side, 0), n);  // keys are [0, n]
+  const int level = pn[i] / 3 + 1;
+  const uint32_t which = uint32_t(codes[lf] >> ((B - 3 * level) & (W - 1))) & 7u;
+  int rt = i;
+  for (int step = 0; step < 31 && ec[rt] == 0; ++step) {
+    const int p = par[rt];
+    rt = uint32_t(p) < uint32_t(n) ? p : 0;
+  }
+  const int bottom = off[rt];
+  if (uint32_t(bottom) >= rows) return false;
+  *slot = uint32_t(bottom) * 8u + which;
+  *leaf = lf;
+  return true;
+}
+
+// Pass 1: every writer claims its slot with atomicMin of -(2 i + side) - 2,
+// so the slot ends holding the claim of the last writer in sequential order
+// (claims are negative, the rows' node links are not); set_leaf's clear of
+// the leaf-mask bit commutes and is applied here.
+template <typename K>
+__global__ void __launch_bounds__(256)
+    k_leaf_claim(const K* __restrict__ codes, const uint8_t* __restrict__ pn,
+                 const uint8_t* __restrict__ hl, const uint8_t* __restrict__ hr,
+                 const int32_t* __restrict__ lc, const int32_t* __restrict__ par,
+                 const int32_t* __restrict__ ec, const int32_t* __restrict__ off,
+                 int32_t* __restrict__ children, int32_t* __restrict__ leaf_mask,
+                 const uint32_t* __restrict__ n_unique, uint32_t rows) {
+  pdl_enter();
+  const uint32_t nu = *n_unique;
+  if (nu < 3 || nu == RW_COUNT_UNSET) return;
+  const int n = int(nu - 1);
+  for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < n; i += int(gridDim.x * blockDim.x))
+    for (int side = 0; side < 2; ++side) {
+      uint32_t slot;
+      int leaf;
+      if (!leaf_target<K>(i, side, n, codes, pn, hl, hr, lc, par, ec, off, rows, &slot, &leaf))
+        continue;
+      atomicMin(children + slot, int(-(int64_t(2 * i + side) + 2)));
+      atomicAnd(leaf_mask + slot / 8u, ~(1 << (slot & 7u)));
+    }
+}
+
+// Pass 2: the writer whose claim survived stores its leaf index.
+template <typename K>
+__global__ void __launch_bounds__(256)
+    k_leaf_write(const K* __restrict__ codes, const uint8_t* __restrict__ pn,
+                 const uint8_t* __restrict__ hl, const uint8_t* __restrict__ hr,
+                 const int32_t* __restrict__ lc, const int32_t* __restrict__ par,
+                 const int32_t* __restrict__ ec, const int32_t* __restrict__ off,
+                 int32_t* __restrict__ children, const uint32_t* __restrict__ n_unique,
+                 uint32_t rows) {
+  pdl_enter();
+  const uint32_t nu = *n_unique;
+  if (nu < 3 || nu == RW_COUNT_UNSET) return;
+  const int n = int(nu - 1);
+  for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < n; i += int(gridDim.x * blockDim.x))
+    for (int side = 0; side < 2; ++side) {
+      uint32_t slot;
+      int leaf;
+      if (!leaf_target<K>(i, side, n, codes, pn, hl, hr, lc, par, ec, off, rows, &slot, &leaf))
+        continue;
+      // a loser reads the winner's claim or its leaf index, never its own claim
+      if (children[slot] == int(-(int64_t(2 * i + side) + 2))) children[slot] = leaf;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 
@@ -1416,6 +1521,34 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
 
 cudaError_t launch_unique(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
   return b.key_bits == 32 ? unique_t<uint32_t>(b, sc, pl, s) : unique_t<uint64_t>(b, sc, pl, s);
+}
+
+cudaError_t launch_prefix_shift(const Bufs& b, const Scratch& sc, const Plan& pl,
+                                cudaStream_t s) {
+  if (pl.seg.count != 1) return cudaErrorInvalidValue;
+  launch_pdl(k_prefix_shift, std::max(1, sc.num_sms * 4), 256, 0, s, b.prefix_n, pl.n_unique);
+  return cudaGetLastError();
+}
+
+namespace {
+template <typename K>
+cudaError_t leaf_links_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s) {
+  const K* codes = static_cast<const K*>(b.keys);
+  const int grid = std::max(1, sc.num_sms * 4);
+  launch_pdl(k_leaf_claim<K>, grid, 256, 0, s, codes, b.prefix_n, b.hl, b.hr, b.lc, b.parents,
+             b.edge_count, b.edge_offset, b.children, b.leaf_mask, pl.n_unique,
+             pl.oct_capacity);
+  launch_pdl(k_leaf_write<K>, grid, 256, 0, s, codes, b.prefix_n, b.hl, b.hr, b.lc, b.parents,
+             b.edge_count, b.edge_offset, b.children, pl.n_unique, pl.oct_capacity);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_leaf_links(const Bufs& b, const Scratch& sc, const Plan& pl,
+                              cudaStream_t s) {
+  if (pl.seg.count != 1) return cudaErrorInvalidValue;
+  return b.key_bits == 32 ? leaf_links_t<uint32_t>(b, sc, pl, s)
+                          : leaf_links_t<uint64_t>(b, sc, pl, s);
 }
 
 cudaError_t launch_unique_raw(const void* sorted, void* out, uint32_t n, int key_bits,

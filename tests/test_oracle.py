@@ -159,3 +159,81 @@ def test_oracle_generators_equal_the_library(rw, oracle, kind, kw):
         want = rw.generate_points(n, kind, seed, **kw)
         got = oracle.generate_points(n, kind, seed, **kw)
         assert got.tobytes() == want.tobytes(), (kind, n, seed)
+
+
+def _oracle_linked(oracle, pts, **kw):
+    from oracle import OPT_LINK_LEAVES
+    return oracle.run(pts, options=OPT_LINK_LEAVES, **kw)
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_leaf_links_equal_the_reference_function(rw, oracle):
+    """The restated leaf linker equals the reference's own process_link_leaf
+    (func_octree.hpp:114-163) run after the canonical stage 7, on every output,
+    on clouds where the reference's unbounded walk ends."""
+    ref = RefTree()
+    compared = 0
+    for i, (n, kind) in enumerate(((307200, "appdata"), (50000, "uniform"), (65537, "gauss"),
+                                   (4096, "gauss"), (200000, "uniform"))):
+        if kind == "appdata":
+            pts = ref.default_points(n)
+        elif kind == "uniform":
+            pts = rw.generate_points(n, rw.GEN_UNIFORM, 900 + i)
+        else:
+            pts = rw.generate_points(n, rw.GEN_GAUSSIAN_MIXTURE, 900 + i, n_components=6,
+                                     sigma_lo=2.0, sigma_hi=20.0)
+        want = ref.canonical(pts, link_leaves=True)
+        if want.status == 4:
+            continue
+        assert want.status == ORC_OK
+        got = _oracle_linked(oracle, pts)
+        assert compare(got, want) == [], (n, kind)
+        # the links did change the octree relative to the default contract
+        plain = oracle.run(pts)
+        assert plain.trimmed()["children"].tobytes() != got.trimmed()["children"].tobytes()
+        compared += 1
+    assert compared >= 3
+
+
+def _octree_is_nested(res, key_bits):
+    """Geometric check of an octree: every child link (node mask bit set)
+    names a row whose cell is half its parent's and lies in the parent's
+    octant `which`; returns the number of violations.  Row 0 is left out as a
+    parent: the reference's layout gives it the root's links but the corner
+    and cell size of the first chain node (edge offset 0), which overwrite the
+    root's initialisation (07_octree.cu:188-198 then func_octree.hpp:62-87)."""
+    t = res.trimmed()
+    ch, mask, corner, cell = t["children"], t["child_node_mask"], t["corner"], t["cell_size"]
+    bad = 0
+    for p in range(1, t["n_octree_nodes"]):
+        for w in range(8):
+            if not (mask[p] >> w) & 1:
+                continue
+            c = ch[p, w]
+            half = cell[p] / 2
+            if cell[c] != half:
+                bad += 1
+                continue
+            for a in range(3):
+                lo = corner[p, a] + (half if (w >> a) & 1 else 0)
+                if corner[c, a] != lo:
+                    bad += 1
+                    break
+    return bad
+
+
+def test_geometric_delta_gives_a_nested_octree(rw, oracle):
+    """With the clz - 2 delta every octree link is geometrically exact (a
+    child cell is the parent's octant at half its size); the reference's
+    clz - 1 shifts levels and breaks that on ordinary clouds.  64-bit keys
+    are unchanged by the option (their clz - 1 is already exact)."""
+    from oracle import OPT_GEOMETRIC_DELTA
+    pts = rw.generate_points(20000, rw.GEN_UNIFORM, 77)
+    geo = oracle.run(pts, options=OPT_GEOMETRIC_DELTA)
+    assert geo.status == ORC_OK
+    assert _octree_is_nested(geo, 32) == 0
+    assert _octree_is_nested(oracle.run(pts), 32) > 0
+    a = oracle.run(pts, key_bits=64)
+    b = oracle.run(pts, key_bits=64, options=OPT_GEOMETRIC_DELTA)
+    assert compare(a, b) == []
+    assert _octree_is_nested(a, 64) == 0
