@@ -58,6 +58,10 @@ def parse_args():
                    help="skip the batched and learned forms in the default line")
     # internal: time the reference's CPU path in a child process (see ref_time_isolated)
     p.add_argument("--ref-time-child", action="store_true", help=argparse.SUPPRESS)
+    # internal: time the reference's CUDA path in a child process (see ref_cuda_isolated)
+    p.add_argument("--ref-cuda-child", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--no-ref-cuda", action="store_true",
+                   help="skip timing the reference's own CUDA path")
     p.add_argument("--ref-threads", type=int, default=0, help=argparse.SUPPRESS)
     p.add_argument("--ref-iters", type=int, default=1, help=argparse.SUPPRESS)
     return p.parse_args()
@@ -529,6 +533,46 @@ def ref_time_isolated(a, seed, iters):
     return out["ms"], out["cores"]
 
 
+def ref_cuda_child(a):
+    """Child side of ref_cuda_isolated: the same cloud through the
+    reference's own CUDA stages 1-7 (oracle/_ref/libref_tree_cuda.so)."""
+    from oracle import RefTreeCuda
+    pts = make_points_checker(a.n, a.dist, a.seed)
+    out = RefTreeCuda().time(pts, a.ref_iters)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def ref_cuda_isolated(a, warmup=2, iters=10):
+    """The reference's CUDA path (cuda::run_stage1..7, pipe_main_baseline.cpp:
+    55-92, compiled for sm_100a) on this workload's cloud, in a child process
+    on the same GPU: median wall ms per run of its seven synchronous stages.
+    32-bit keys and sizes that are multiples of 1024 only (its k_FindDups
+    reads whole 1,024-key tiles).  A comparison point, not a parity check:
+    the driver copies the sorted keys into the buffer its stage 3 reads (the
+    buffer contract its dispatcher does not honour) and runs its stage 4 and
+    stage 7 only after device-side checks of their inputs."""
+    from oracle import ref_cuda_available
+    if a.key_bits != 32 or a.n % 1024 or not ref_cuda_available():
+        return {"unavailable": "32-bit keys, n a multiple of 1024 and oracle/_ref built only"}
+    cmd = [sys.executable, os.path.abspath(__file__), "--ref-cuda-child", "--n", str(a.n),
+           "--dist", a.dist, "--seed", str(a.seed), "--ref-iters", str(warmup + iters)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference's CUDA path did not finish in 10 minutes"}
+    if r.returncode != 0:
+        return {"unavailable": f"the reference's CUDA path exited with {r.returncode}: "
+                               f"{r.stderr.strip()[-300:]}"}
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    ms = out.pop("ms")[warmup:]
+    t = statistics.median(ms)
+    out.update({"ms_per_step": round(t, 4), "value": a.n / (t / 1e3), "unit": "points/s",
+                "sample": f"median of {iters} runs after {warmup} warm-up runs, wall time of "
+                          f"its seven synchronous stages (device-side checks excluded)"})
+    return out
+
+
 def port_time(pts, a, iters):
     from oracle import Oracle
     orc = Oracle()
@@ -571,6 +615,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.ref_time_child:
         return ref_time_child(a)
+    if a.ref_cuda_child:
+        return ref_cuda_child(a)
     if a.impl == "reference":
         return run_reference(a, rank)
 
@@ -743,6 +789,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(rw, pts, a)
+    ref_cuda = None
+    if rank == 0 and world == 1 and not a.no_ref_cuda:
+        ref_cuda = ref_cuda_isolated(a)
 
     forms = None
     if rank == 0 and not a.no_forms:
@@ -768,6 +817,7 @@ def main():
         "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
                               "frac": round(pipe_gbs / hbm, 4)},
         "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
+        "reference_cuda": ref_cuda,
         "clocks": clocks.summary(), "gpu_launches": (11 + passes) * a.steps,
         "forms": forms,
     }

@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_tree.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libref_tree_cuda.so")
 
 ORC_OK, ORC_ERR_ARG, ORC_ERR_DEGENERATE, ORC_ERR_CAPACITY = 0, 1, 2, 3
 
@@ -316,6 +317,38 @@ class RefTree:
         r.n_unique, r.n_brt_nodes = o.n_unique, o.n_brt_nodes
         r.n_octree_nodes = o.n_octree_nodes
         return r
+
+
+def ref_cuda_available(path: str = REF_CUDA_SO) -> bool:
+    return os.path.exists(path)
+
+
+class RefTreeCuda:
+    """The reference's own CUDA tree path (cuda::run_stage1..7 compiled for
+    sm_100a, _ref/libref_tree_cuda.so, driven by ref_cuda_driver.cu): a timing
+    comparison point on the same GPU, not a checker."""
+
+    def __init__(self, path: str = REF_CUDA_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        self.lib = ctypes.CDLL(path)
+
+    def time(self, points: np.ndarray, iters: int) -> dict:
+        """Wall ms of `iters` runs (n a multiple of 1024) and what ran."""
+        points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+        n = points.shape[0]
+        ms = np.zeros(iters, np.float64)
+        info = np.zeros(6, np.uint32)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.refcu_time(_ptr(points), ctypes.c_uint32(n), ctypes.c_int(iters),
+                                 _ptr(ms), _ptr(info), err, ctypes.c_int(512))
+        if rc:
+            raise RuntimeError(f"refcu_time: status {rc} {err.value.decode()}")
+        return {"ms": ms.tolist(), "all_stages_ran": bool(info[0]),
+                "rows_out_of_range": int(info[1]), "parents_out_of_range": int(info[2]),
+                "n_unique": int(info[3]),
+                "n_octree_nodes": None if info[4] == 0xFFFFFFFF else int(info[4]),
+                "stage4_input_unsorted": bool(info[5])}
 
 
 def compare(a: TreeResult, b: TreeResult) -> list[str]:

@@ -1,0 +1,194 @@
+// Test infrastructure, not product code: a driver around the reference's OWN
+// CUDA tree path (apps/tree/cuda/*.cu, compiled for sm_100a from its sources
+// by oracle/Makefile into _ref/), so that it can be timed on the same GPU as
+// this project's pipeline.  It is a second comparison point only, not a
+// parity check.
+//
+// The loop body is pipe_main_baseline.cpp:55-92 (cuda::run_stage1..7 on a
+// managed-memory AppData and a cuda::ImStorage, one blocking stream, each
+// stage synchronising as the reference's do), with one fix and two checks:
+//
+//   - the fix: the reference's sort leaves the sorted keys in u_morton_keys
+//     after its four ping-pong passes, but its stage 3 reads
+//     u_morton_keys_alt (cu_dispatcher.cu:550-607), which then holds keys
+//     sorted on their low 24 bits only.  On such keys its stage 4 meets
+//     nodes with direction 0 and empty ranges, where log2_ceil_u32(0)
+//     (04_radix_tree.cu:23-31) shifts by a negative count - undefined
+//     behaviour that bounds a loop.  The driver therefore copies the sorted
+//     keys into u_morton_keys_alt after stage 2, as the buffer contract of
+//     app_data.hpp:139-150 says they should be (the copy is timed);
+//   - before stage 4, a project-written kernel checks on the device that its
+//     input keys are strictly increasing (stages 4-7 are skipped otherwise);
+//   - before stage 7 (k_MakeOctNodes, 07_octree.cu:175-226), which writes
+//     octree rows at offsets the earlier stages derive, a project-written
+//     kernel checks every row it would touch (the chain rows [off[i],
+//     off[i] + count[i]) and the parent row of the bounded walk,
+//     func_octree.hpp:89-99) and every parent index it would follow; stage 7
+//     runs only when all are in range.
+// The checks are outside the timed spans.
+//
+// Only sizes that are multiples of 1024 are accepted: the reference's
+// k_FindDups loads whole 1,024-key tiles without a tail check
+// (agents/unique_agent.cuh:58).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory_resource>
+
+#include "app_data.hpp"
+#include "cuda/cu_dispatcher.cuh"
+#include "cuda/im_storage.cuh"
+#include "redwood/cuda/cu_mem_resource.cuh"
+#include "redwood/cuda/helpers.cuh"
+
+namespace {
+
+// flags[0]: rows out of range, flags[1]: parent indices out of range
+__global__ void k_check_stage7(const int* __restrict__ edge_offset,
+                               const int* __restrict__ edge_count,
+                               const int* __restrict__ parents, int n_brt,
+                               int n_input, int rows, unsigned* __restrict__ flags) {
+  for (int i = 1 + int(blockIdx.x * blockDim.x + threadIdx.x); i < n_brt;
+       i += int(gridDim.x * blockDim.x)) {
+    const int nn = edge_count[i];
+    if (nn <= 0) continue;  // stage 7 writes nothing for this node
+    const long long first = edge_offset[i];
+    if (first < 0 || first + nn > rows) {
+      atomicAdd(flags, 1u);
+      continue;
+    }
+    int rt = parents[i];
+    if (rt < 0 || rt >= n_input) {
+      atomicAdd(flags + 1, 1u);
+      continue;
+    }
+    bool ok = true;
+    for (int counter = 0; edge_count[rt] == 0;) {
+      rt = parents[rt];
+      if (rt < 0 || rt >= n_input) {
+        ok = false;
+        break;
+      }
+      if (++counter > 30) break;
+    }
+    if (!ok) {
+      atomicAdd(flags + 1, 1u);
+      continue;
+    }
+    const int top = edge_offset[rt];
+    if (top < 0 || top >= rows) atomicAdd(flags, 1u);
+  }
+}
+
+// flags[0] += 1 for every i in [1, n) with keys[i - 1] >= keys[i]
+__global__ void k_check_increasing(const unsigned* __restrict__ keys, int n,
+                                   unsigned* __restrict__ flags) {
+  for (int i = 1 + int(blockIdx.x * blockDim.x + threadIdx.x); i < n;
+       i += int(gridDim.x * blockDim.x))
+    if (keys[i - 1] >= keys[i]) atomicAdd(flags, 1u);
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+      .count();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Times `iters` runs of the reference's cuda::run_stage1..7 on the cloud
+// pts[4 n] (copied into the AppData's managed input once).  per_iter_ms gets
+// each run's wall time (the stages that ran, checks excluded).  info[0] = 1
+// when every stage ran in every run, info[1] = octree rows out of range found
+// by the stage-7 check (last run), info[2] = parent indices out of range,
+// info[3] = the reference's n_unique, info[4] = its n_octree_nodes (last
+// run), info[5] = 1 when stage 4's input was not strictly increasing.
+// Returns 0, 1 for bad arguments, 2 for a CUDA error (text in err).
+int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uint32_t* info,
+               char* err, int err_len) {
+  if (!pts || n < 1024 || n % 1024 != 0 || iters < 1 || !per_iter_ms || !info) return 1;
+  try {
+    cudaStream_t stream;
+    CUDA_CHECK(cudaStreamCreate(&stream));
+    cuda::CudaMemoryResource mr;
+    {
+      AppData app(&mr, n);
+      std::memcpy(app.u_input_points.data(), pts, size_t(16) * n);
+      cuda::ImStorage im(static_cast<int>(n));
+      unsigned* flags = nullptr;
+      CUDA_CHECK(cudaMalloc(&flags, 2 * sizeof(unsigned)));
+      const int rows = static_cast<int>(app.oct.u_children.size() / 8);
+      bool all_ran = true;
+      unsigned host_flags[2] = {0, 0};
+      info[5] = 0;
+      uint32_t last_m = 0xffffffffu;
+      auto check = [&](auto launch) {
+        CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned), stream));
+        launch();
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaMemcpyAsync(host_flags, flags, sizeof host_flags,
+                                   cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        return host_flags[0] == 0 && host_flags[1] == 0;
+      };
+      for (int it = 0; it < iters; ++it) {
+        auto t0 = std::chrono::steady_clock::now();
+        cuda::run_stage1(app, stream);
+        cuda::run_stage2(app, im, stream);
+        CUDA_CHECK(cudaMemcpyAsync(app.u_morton_keys_alt.data(), app.u_morton_keys.data(),
+                                   size_t(4) * n, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        cuda::run_stage3(app, im, stream);
+        double ms = ms_since(t0);
+        const int nu = static_cast<int>(app.get_n_unique());
+        const bool sorted = nu >= 3 && nu <= static_cast<int>(n) && check([&] {
+          k_check_increasing<<<148 * 4, 256, 0, stream>>>(app.u_morton_keys.data(), nu, flags);
+        });
+        if (!sorted) {
+          all_ran = false;
+          info[5] = 1;
+          per_iter_ms[it] = ms;
+          continue;
+        }
+        t0 = std::chrono::steady_clock::now();
+        cuda::run_stage4(app, stream);
+        cuda::run_stage5(app, stream);
+        cuda::run_stage6(app, stream);
+        ms += ms_since(t0);
+        last_m = app.get_n_octree_nodes();
+        const bool rows_ok = check([&] {
+          k_check_stage7<<<148 * 4, 256, 0, stream>>>(
+              app.u_edge_offset.data(), app.u_edge_count.data(), app.brt.u_parents.data(),
+              static_cast<int>(app.get_n_brt_nodes()), static_cast<int>(n), rows, flags);
+        });
+        if (rows_ok) {
+          t0 = std::chrono::steady_clock::now();
+          cuda::run_stage7(app, stream);
+          ms += ms_since(t0);
+        } else {
+          all_ran = false;
+        }
+        per_iter_ms[it] = ms;
+      }
+      info[0] = all_ran ? 1u : 0u;
+      info[1] = host_flags[0];
+      info[2] = host_flags[1];
+      info[3] = app.get_n_unique();
+      info[4] = last_m;
+      CUDA_CHECK(cudaFree(flags));
+    }
+    CUDA_CHECK(cudaStreamDestroy(stream));
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) {
+      std::strncpy(err, e.what(), size_t(err_len) - 1);
+      err[err_len - 1] = '\0';
+    }
+    return 2;
+  }
+  return 0;
+}
+
+}  // extern "C"
