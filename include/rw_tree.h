@@ -372,9 +372,13 @@ int rw_tree_learned_set_params(rw_tree_learned* learned, const float* params, in
                                int32_t group);
 /* Context group size alone (for rw_tree_learned_features); default 4. */
 int rw_tree_learned_set_group(rw_tree_learned* learned, int32_t group);
-/* Sorts d_keys[0, n) (16-byte aligned) into d_sorted.  `fallback_im`
- * (storage for n keys) runs the onesweep sort when needed; stats may be NULL.
- * Synchronises once (the bucket plan decides the path). */
+/* Sorts d_keys[0, n) (16-byte aligned) into d_sorted.  With `fallback_im`
+ * (storage for n keys) the call is asynchronous on `stream` and capturable in
+ * a CUDA graph: the bucket sort and a onesweep sort on fallback_im are both
+ * enqueued, and the plan's overflow word, on the device, lets exactly one of
+ * them write d_sorted.  `stats` (may be NULL) is filled after one wait for
+ * the stream.  Without fallback_im the call waits for the plan and returns
+ * RW_ERR_CAPACITY on an overflow (and for n < 65,536) instead of sorting. */
 int rw_tree_learned_sort(rw_tree_learned* learned, const uint32_t* d_keys, uint32_t* d_sorted,
                          uint32_t n, int32_t mode, rw_tree_im_storage* fallback_im,
                          rw_stream_t stream, rw_tree_learned_stats* stats);
@@ -392,8 +396,8 @@ int rw_tree_learned_bucket_counts(rw_tree_learned* learned, const uint32_t* d_ke
 /* Stage 2 of this scratch's pipeline (rw_tree_run_stage2 and
  * rw_tree_pipeline_enqueue) sorts with `learned` in `mode` instead of the
  * onesweep sort; NULL restores onesweep.  32-bit keys only; `learned` must
- * serve n_input keys and outlive its use here.  The pipeline then waits once
- * for the learned sort's bucket plan inside rw_tree_pipeline_enqueue, and
+ * serve n_input keys and outlive its use here.  The pipeline stays
+ * asynchronous and capturable (the fallback is decided on the device), and
  * rw_tree_pipeline_profile reports "morton,learned_sort,..." (7 entries).
  * The output is bit-identical either way. */
 int rw_tree_im_storage_set_learned(rw_tree_im_storage* im, rw_tree_learned* learned,

@@ -155,6 +155,24 @@ int sync_status(rw_tree_im_storage* im, cudaStream_t s) {
 
 namespace rwt {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int sort_enqueue_gated(rw_tree_im_storage* im, const void* keys, void* out, uint32_t n,
+                       const uint32_t* gate, bool clear, cudaStream_t s) {
+  rw_tree_app_data app;
+  rw_tree_app_data_init(&app, n, im ? im->key_bits : 32);
+  app.u_morton_keys = const_cast<void*>(keys);
+  app.u_morton_keys_alt = out;
+  if (int rc = check(&app, im, kKeys | kAlt)) return rc;
+  if (clear)
+    if (int rc = clear_all(im, s)) return rc;
+  const auto b = bufs_of(app, im);
+  auto sc = scratch_of(im);
+  sc.gate = gate;
+  const auto pl = plan_of(app, im);
+  RW_CUDA(launch_keys(b, sc, pl, false, true, s));
+  RW_CUDA(launch_sort_passes(b, sc, pl, s));
+  return RW_OK;
+}
 }  // namespace rwt
 
 extern "C" {
@@ -479,10 +497,9 @@ int enqueue_impl(rw_tree_app_data* app, rw_tree_im_storage* im, cudaStream_t s,
     // waits for its bucket plan once, and falls back to onesweep on `im`)
     RW_CUDA(rwt::launch_keys(b, sc, pl, true, false, s));
     RW_CUDA(mark());
-    if (int rc = rw_tree_learned_sort(im->learned, static_cast<const uint32_t*>(b.keys),
-                                      static_cast<uint32_t*>(b.alt), app->n_input,
-                                      im->learned_mode, im, reinterpret_cast<rw_stream_t>(s),
-                                      &im->learned_stats))
+    if (int rc = rwt::learned_sort_enqueue(im->learned, static_cast<const uint32_t*>(b.keys),
+                                           static_cast<uint32_t*>(b.alt), app->n_input,
+                                           im->learned_mode, im, false, s))
       return rc;
     RW_CUDA(mark());
   } else {
@@ -580,6 +597,7 @@ int rw_tree_pipeline_finish(rw_tree_app_data* app, rw_tree_im_storage* im,
                             rw_stream_t stream) {
   if (!app || !im) return RW_ERR_ARG;
   RW_CUDA(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+  if (im->learned) rwt::learned_last_stats(im->learned, &im->learned_stats);
   const rwt::DevStatus st = *im->h_status;
   app->n_unique = st.n_unique;
   app->n_brt_nodes = st.n_unique - 1;

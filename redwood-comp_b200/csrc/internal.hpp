@@ -118,6 +118,10 @@ struct Scratch {
   DevStatus* status = nullptr;
   // polls of a look-back wait before it gives up with RW_ERR_TIMEOUT
   uint32_t spin_limit = kSpinLimit;
+  // when set, the sort's kernels (digit histograms, set-up, passes) do their
+  // work only if *gate != 0, read on the device: a fallback sort enqueued
+  // ahead of the decision that needs it
+  const uint32_t* gate = nullptr;
   // tree_far_cap entries of 16 bytes: radix-tree gaps left to the far search
   // (gap, segment: 8 bytes each), then the octree's far links (16 bytes each)
   uint32_t* tree_far = nullptr;
@@ -156,6 +160,23 @@ cudaError_t launch_keys(const Bufs& b, const Scratch& sc, const Plan& pl, bool e
 // kernel and one after each pass (profiling only).
 cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,
                                cudaStream_t s, cudaEvent_t* marks = nullptr);
+// The onesweep sort of keys[0, n) into out on `im`'s scratch, with every
+// kernel gated on *gate (see Scratch::gate); `clear` zeroes the scratch's
+// zero region first (not needed when a pipeline cleared it and has not used
+// it since).  For the learned sort's device-decided fallback.
+int sort_enqueue_gated(rw_tree_im_storage* im, const void* keys, void* out, uint32_t n,
+                       const uint32_t* gate, bool clear, cudaStream_t s);
+
+// The learned-CDF sort of keys[0, n) into sorted, enqueued without any host
+// wait: the bucket sort and a gated onesweep fallback on fallback_im (needed)
+// are both enqueued and the plan's overflow word picks one on the device.
+// The plan is copied to pinned host memory; learned_last_stats reads it once
+// the stream has passed this sort.
+int learned_sort_enqueue(rw_tree_learned* L, const uint32_t* keys, uint32_t* sorted, uint32_t n,
+                         int32_t mode, rw_tree_im_storage* fallback_im, bool clear_fallback,
+                         cudaStream_t s);
+void learned_last_stats(const rw_tree_learned* L, rw_tree_learned_stats* out);
+
 // Test hook of the bounded look-back wait: the digit histograms of b.keys,
 // then pass 0 of the sort into b.alt with tile 0 left out, so that every
 // other tile's look-back waits on a row nothing publishes and gives up after

@@ -35,8 +35,10 @@ template <typename K, int D, bool HIST, bool ENCODE, bool POW2>
 __global__ void __launch_bounds__(256)
     k_keys_pass(const float4* __restrict__ pts, K* __restrict__ keys, SegTable seg,
                 TileMap map, uint32_t tiles_per_cta, float min_coord, float range,
-                float inv_range, uint32_t* __restrict__ ghist) {
+                float inv_range, uint32_t* __restrict__ ghist,
+                const uint32_t* __restrict__ gate) {
   pdl_enter();
+  if (gate && *gate == 0) return;  // a gated sort that is not needed this run
   constexpr int RADIX = 1 << D;
   // the sort's passes: ceil(code bits / D), as the storage computes them
   constexpr int P = (KeyTraits<K>::kCodeBits + D - 1) / D;
@@ -120,8 +122,10 @@ __global__ void __launch_bounds__(256)
 template <int D>
 __global__ void __launch_bounds__(256)
     k_sort_init(const uint32_t* __restrict__ ghist, uint32_t* __restrict__ desc,
-                SegTable seg, TileMap map, int passes, uint32_t rows_per_pass) {
+                SegTable seg, TileMap map, int passes, uint32_t rows_per_pass,
+                const uint32_t* __restrict__ gate) {
   pdl_enter();
+  if (gate && *gate == 0) return;
   constexpr int RADIX = 1 << D;
   constexpr int R = (RADIX + 255) / 256;
   static_assert(R * 256 >= RADIX, "every digit needs an offset");
@@ -178,8 +182,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
               uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st,
-              uint32_t spin_limit) {
+              uint32_t spin_limit, const uint32_t* __restrict__ gate) {
   pdl_enter();
+  if (gate && *gate == 0) return;  // every tile of the pass returns: no look-back waits
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
   constexpr int RADIX = C::RADIX, NW = C::NW, TILE = C::TILE;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -341,7 +346,7 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
     if (smem > 48 * 1024)                                                            \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
     launch_pdl(kern, grid, 256, smem, s, b.points, keys, pl.seg, pl.point_map, per, b.min_coord, \
-                                 b.range, inv, sc.ghist);                            \
+                                 b.range, inv, sc.ghist, sc.gate);                   \
   } while (0)
   if (encode && hist) RWT_KEYS_LAUNCH(true, true);
   else if (encode) RWT_KEYS_LAUNCH(false, true);
@@ -359,7 +364,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   const uint32_t tiles = pl.sort_map.n_tiles;
   if (tiles + pl.seg.count > sc.sort_rows) return cudaErrorInvalidValue;
   launch_pdl(k_sort_init<D>, pl.seg.count * sc.passes, 256, 0, s, sc.ghist, sc.sort_desc, pl.seg,
-                                                          pl.sort_map, sc.passes, sc.sort_rows);
+                                                          pl.sort_map, sc.passes, sc.sort_rows, sc.gate);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
@@ -377,7 +382,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
     if (e != cudaSuccess) return e;
     launch_pdl(kern, tiles - 1, THREADS, C::kSmem, s, static_cast<const K*>(keys), alt, pl.seg,
                pl.sort_map, 0, sc.sort_desc, sc.tile_ctr + kCtrSortBase, sc.status,
-               probe_spins);
+               probe_spins, static_cast<const uint32_t*>(nullptr));
     return cudaGetLastError();
   }
   const K* src = keys;
@@ -387,7 +392,7 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
       launch_pdl(kern, tiles, THREADS, C::kSmem, s, 
           src, dst, pl.seg, pl.sort_map, p * D,
           sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
-          sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit);
+          sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit, sc.gate);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (marks) cudaEventRecord(marks[1 + p], s);

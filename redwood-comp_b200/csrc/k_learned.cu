@@ -30,8 +30,11 @@
 //     run a stable LSD in shared memory over the bits they span, with the
 //     onesweep passes' warp ranking; a bucket above one CTA's capacity is
 //     sorted by its CTA in chunks through global memory.  A region that
-//     overflowed sends the whole input to the onesweep sort (decided on the
-//     host, which reads the plan).
+//     overflowed sends the whole input to the onesweep sort, decided on the
+//     device: the onesweep kernels are enqueued behind the bucket sort with a
+//     gate on the plan's overflow word (they return at once when it is 0, the
+//     bucket sort returns at once when it is 1), so no host wait is needed
+//     and the whole sort can be captured in a CUDA graph.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -710,8 +713,9 @@ __device__ __noinline__ void bucket_sort_big(uint32_t* __restrict__ a, uint32_t 
 __global__ void __launch_bounds__(kBsThreads, 1)
     k_bucket_sort(uint32_t* __restrict__ region, uint32_t cap, const uint32_t* __restrict__ counts,
                   const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ order,
-                  uint32_t* __restrict__ out) {
+                  const LearnedPlan* __restrict__ plan, uint32_t* __restrict__ out) {
   pdl_enter();
+  if (plan->fallback) return;  // a region overflowed: the gated onesweep sort writes `out`
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t bk = order[blockIdx.x];
   const uint32_t cnt = counts[bk];
@@ -826,6 +830,36 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 }  // namespace
 
+namespace rwt {
+
+int learned_sort_enqueue(rw_tree_learned* L, const uint32_t* keys, uint32_t* sorted, uint32_t n,
+                         int32_t mode, rw_tree_im_storage* fallback_im, bool clear_fallback,
+                         cudaStream_t s) {
+  if (n < kSample) {  // too few keys to sample: the onesweep sort, known on the host
+    // the plan records the fallback, in stream order like a sampled run's
+    RWL_CUDA(cudaMemsetAsync(L->d_plan, 0, sizeof(LearnedPlan), s));
+    RWL_CUDA(cudaMemsetAsync(&L->d_plan->fallback, 1, 1, s));
+    RWL_CUDA(cudaMemcpyAsync(L->h_plan, L->d_plan, sizeof(LearnedPlan), cudaMemcpyDeviceToHost,
+                             s));
+    return sort_enqueue_gated(fallback_im, keys, sorted, n, nullptr, clear_fallback, s);
+  }
+  if (int rc = front_half(L, keys, n, mode == RW_LEARNED_MLP, false, s)) return rc;
+  if (int rc = scatter_and_plan(L, keys, n, s)) return rc;
+  launch_pdl(k_bucket_sort, kBuckets, kBsThreads, kBsSmem, s, L->d_region, region_cap(n),
+             L->d_cursor, L->d_offsets, L->d_order, L->d_plan, sorted);
+  RWL_CUDA(cudaGetLastError());
+  return sort_enqueue_gated(fallback_im, keys, sorted, n, &L->d_plan->fallback, clear_fallback, s);
+}
+
+void learned_last_stats(const rw_tree_learned* L, rw_tree_learned_stats* out) {
+  std::memset(out, 0, sizeof *out);
+  out->max_bucket = L->h_plan->max_count;
+  out->big_buckets = L->h_plan->n_big;
+  out->fell_back = L->h_plan->fallback;
+}
+
+}  // namespace rwt
+
 extern "C" {
 
 int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
@@ -933,29 +967,27 @@ int rw_tree_learned_sort(rw_tree_learned* L, const uint32_t* d_keys, uint32_t* d
     return RW_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (stats) std::memset(stats, 0, sizeof *stats);
-  bool fallback = n < rwt::kSample;
-  if (!fallback) {
+  if (!fallback_im) {
+    // no scratch for a fallback: the plan is read on the host and an
+    // overflow is reported instead of sorted
+    if (n < rwt::kSample) return RW_ERR_CAPACITY;
     if (int rc = front_half(L, d_keys, n, mode == RW_LEARNED_MLP, false, s)) return rc;
     if (int rc = scatter_and_plan(L, d_keys, n, s)) return rc;
-    RWL_CUDA(cudaStreamSynchronize(s));  // the plan decides the path
-    fallback = L->h_plan->fallback != 0;
-    if (stats) {
-      stats->max_bucket = L->h_plan->max_count;
-      stats->big_buckets = L->h_plan->n_big;
-    }
+    RWL_CUDA(cudaStreamSynchronize(s));
+    if (stats) rwt::learned_last_stats(L, stats);
+    if (L->h_plan->fallback) return RW_ERR_CAPACITY;
+    rwt::launch_pdl(rwt::k_bucket_sort, rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s,
+        L->d_region, rwt::region_cap(n), L->d_cursor, L->d_offsets, L->d_order, L->d_plan,
+        d_sorted);
+    RWL_CUDA(cudaGetLastError());
+    return RW_OK;
   }
-  if (fallback) {
-    if (!fallback_im) return RW_ERR_CAPACITY;
-    rw_tree_app_data app;
-    rw_tree_app_data_init(&app, n, 32);
-    app.u_morton_keys = const_cast<uint32_t*>(d_keys);
-    app.u_morton_keys_alt = d_sorted;
-    if (stats) stats->fell_back = 1;
-    return rw_tree_sort_enqueue(&app, fallback_im, stream);
+  if (int rc = rwt::learned_sort_enqueue(L, d_keys, d_sorted, n, mode, fallback_im, true, s))
+    return rc;
+  if (stats) {
+    RWL_CUDA(cudaStreamSynchronize(s));
+    rwt::learned_last_stats(L, stats);
   }
-  rwt::launch_pdl(rwt::k_bucket_sort, rwt::kBuckets, rwt::kBsThreads, rwt::kBsSmem, s, 
-      L->d_region, rwt::region_cap(n), L->d_cursor, L->d_offsets, L->d_order, d_sorted);
-  RWL_CUDA(cudaGetLastError());
   return RW_OK;
 }
 

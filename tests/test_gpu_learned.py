@@ -200,3 +200,37 @@ def test_trained_network_gains_over_sample_quantiles(rw):
           f"max/mean: mlp {mx_m:.3f} vs {mx_s:.3f}")
     assert cv_m < 0.97 * cv_s
     assert mx_m < mx_s
+
+
+def test_learned_pipeline_replayed_from_a_cuda_graph(rw, oracle):
+    """With the learned sort in stage 2 the fused pipeline needs no host wait
+    (the overflow fallback is decided on the device), so it captures into a
+    CUDA graph; replays on clouds that take the bucket path and on one whose
+    single dense spot overflows its bucket region (the gated onesweep sort
+    runs instead) are all exact against the oracle."""
+    import torch
+    from redwood_comp_b200 import learned
+    from test_gpu_parity import assert_same
+    n = 1 << 20
+    L = rw.Learned(n)
+    if L.params is None:
+        L.set_params(learned.init_params(1))
+    app = rw.AppData(n, 32, points=learned.mixture_cloud(rw, n, 31_001))
+    im = rw.ImStorage(n, 32)
+    im.set_learned(L, rw.LEARNED_MLP)
+    rw.run_pipeline(app, im)  # first run outside the capture
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rw.pipeline_enqueue(app, im)
+    dense = rw.generate_points(n, rw.GEN_UNIFORM, 31_004)
+    dense[: n // 5] = np.float32(333.25)  # a fifth of the points on one spot
+    for name, pts, fell_back in (("mixture", learned.mixture_cloud(rw, n, 31_002), 0),
+                                 ("dense spot", dense, 1),
+                                 ("mixture again", learned.mixture_cloud(rw, n, 31_003), 0)):
+        app.set_points(pts)
+        g.replay()
+        rw.pipeline_finish(app, im)
+        assert im.learned_stats()["fell_back"] == fell_back, name
+        assert_same(app.results(), oracle.run(pts), f"graph replay {name}")
+    del g
+    im.set_learned(None)
