@@ -87,6 +87,9 @@ typedef struct rw_tree_app_data {
  * key buffer, device-side counts and the error word. */
 typedef struct rw_tree_im_storage rw_tree_im_storage;
 
+/* Opaque scratch of the learned-CDF sort (see its section below). */
+typedef struct rw_tree_learned rw_tree_learned;
+
 /* Octree rows for n points: floor(n * 0.6f) in float (app_data.hpp:13,28). */
 uint32_t rw_tree_octree_capacity(uint32_t n_input);
 
@@ -297,6 +300,14 @@ int rw_tree_batch_set_sort_variant(rw_tree_batch* batch, int32_t idx);
  * every larger cloud).  The autotuner writes these tables. */
 int rw_tree_batch_set_classes(rw_tree_batch* batch, uint32_t n_classes,
                               const uint32_t* max_points, const int32_t* variants);
+/* Stage 2 of every cloud by the learned-CDF sort (32-bit keys), one sort per
+ * cloud enqueued back to back (each decides its onesweep fallback on the
+ * device, on `fallback_im`, so the batch stays capturable); the other stages
+ * stay one launch for the whole batch.  `learned` must serve the largest
+ * cloud, `fallback_im` hold storage for it, and both outlive their use here;
+ * NULL restores the batched onesweep sort.  Outputs are identical either way. */
+int rw_tree_batch_set_learned(rw_tree_batch* batch, rw_tree_learned* learned, int32_t mode,
+                              rw_tree_im_storage* fallback_im);
 /* All stages for every cloud, asynchronous on `stream` (capturable). */
 int rw_tree_batch_enqueue(rw_tree_batch* batch, const rw_tree_batch_buffers* bufs,
                           rw_stream_t stream);
@@ -348,7 +359,6 @@ int rw_tree_sort_lookback_probe(rw_tree_app_data* app, rw_tree_im_storage* im,
  * and each bucket is sorted exactly.  A bucket that overflows its region
  * sends the whole input to the onesweep sort.  The output is the sorted input
  * either way. */
-typedef struct rw_tree_learned rw_tree_learned;
 #define RW_LEARNED_MLP 0
 #define RW_LEARNED_SAMPLE_QUANTILES 1
 #define RW_LEARNED_MLP_PARAMS 5313 /* 16*64 + 64 + 64*64 + 64 + 64 + 1 */

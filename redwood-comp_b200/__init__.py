@@ -105,6 +105,7 @@ EXPORTS = (
     "rw_tree_batch_set_sort_variant", "rw_tree_batch_enqueue", "rw_tree_batch_graph_launch",
     "rw_tree_batch_finish", "rw_tree_batch_set_classes", "rw_tree_sort_enqueue",
     "rw_tree_sort_profile", "rw_tree_sort_lookback_probe", "rw_tree_im_storage_set_options",
+    "rw_tree_batch_set_learned",
     "rw_tree_learned_create", "rw_tree_learned_destroy", "rw_tree_learned_set_params",
     "rw_tree_learned_set_group", "rw_tree_im_storage_set_learned",
     "rw_tree_im_storage_learned_stats", "rw_tree_host_submit", "rw_tree_host_collect",
@@ -535,14 +536,16 @@ class Batch:
         host = np.concatenate([np.ascontiguousarray(c, np.float32).reshape(-1, 4) for c in clouds])
         self.points.copy_(torch.from_numpy(host))
 
-    def set_options(self, options: int) -> None:
-        """OPT_GEOMETRIC_DELTA / OPT_LINK_LEAVES bits (0: the reference's own
-        outputs); see rw_tree_im_storage_set_options."""
-        _check(lib().rw_tree_im_storage_set_options(self._h, ctypes.c_int32(options)),
-               "set_options")
-
     def set_sort_variant(self, idx: int) -> None:
         _check(lib().rw_tree_batch_set_sort_variant(self._h, idx), "batch_set_sort_variant")
+
+    def set_learned(self, learned, mode: int = 0, fallback_im=None) -> None:
+        """Stage 2 of every cloud by the learned-CDF sort (32-bit keys;
+        rw_tree_batch_set_learned); None restores the batched onesweep sort."""
+        self._learned = (learned, fallback_im)  # kept alive while in use
+        _check(lib().rw_tree_batch_set_learned(
+            self._h, learned._h if learned is not None else None, ctypes.c_int32(mode),
+            fallback_im.handle if fallback_im is not None else None), "batch_set_learned")
 
     def set_classes(self, classes) -> None:
         """classes: [(max_points, variant_index), ...] ascending; the last

@@ -59,6 +59,11 @@ struct rw_tree_batch {
 
   uint32_t* h_results = nullptr;  // pinned: n_unique[C], n_octree[C], seg_err[C], status
 
+  // optional learned-CDF sort for stage 2, one sort per cloud (not owned)
+  rw_tree_learned* learned = nullptr;
+  int32_t learned_mode = 0;
+  rw_tree_im_storage* learned_fallback = nullptr;
+
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   rw_tree_batch_buffers graph_bufs{};
@@ -390,6 +395,24 @@ int rw_tree_batch_set_classes(rw_tree_batch* b, uint32_t n_classes, const uint32
   return RW_OK;
 }
 
+int rw_tree_batch_set_learned(rw_tree_batch* b, rw_tree_learned* learned, int32_t mode,
+                              rw_tree_im_storage* fallback_im) {
+  if (!b || (mode != RW_LEARNED_MLP && mode != RW_LEARNED_SAMPLE_QUANTILES)) return RW_ERR_ARG;
+  if (learned) {
+    uint32_t largest = 0;
+    for (uint32_t c = 0; c < b->n_clouds; ++c)
+      largest = std::max(largest, b->h_pt_off[c + 1] - b->h_pt_off[c]);
+    if (b->key_bits != 32 || !fallback_im || rwt::learned_capacity(learned) < largest ||
+        fallback_im->key_bits != 32 || fallback_im->n_cap < largest)
+      return RW_ERR_ARG;
+  }
+  b->learned = learned;
+  b->learned_mode = mode;
+  b->learned_fallback = learned ? fallback_im : nullptr;
+  release_graph(b);  // the captured graph used the other stage 2
+  return RW_OK;
+}
+
 int rw_tree_batch_enqueue(rw_tree_batch* b, const rw_tree_batch_buffers* u, rw_stream_t stream) {
   if (!b) return RW_ERR_ARG;
   if (int rc = check_bufs(u)) return rc;
@@ -398,9 +421,23 @@ int rw_tree_batch_enqueue(rw_tree_batch* b, const rw_tree_batch_buffers* u, rw_s
   const auto sc = scratch_of(b);
   const auto pl = plan_of(b);
   RWB_CUDA(cudaMemsetAsync(b->d_zero, 0, b->zero_bytes, s));
-  RWB_CUDA(rwt::launch_keys(x, sc, pl, true, true, s));
+  if (b->learned) {
+    // stage 1 without the digit histograms, then every cloud's learned sort
+    // (asynchronous: its onesweep fallback is decided on the device), back to
+    // back on the stream
+    RWB_CUDA(rwt::launch_keys(x, sc, pl, true, false, s));
+    const uint32_t* keys = static_cast<const uint32_t*>(x.keys);
+    uint32_t* alt = static_cast<uint32_t*>(x.alt);
+    for (uint32_t c = 0; c < b->n_clouds; ++c) {
+      const uint32_t p0 = b->h_pt_off[c], nc = b->h_pt_off[c + 1] - p0;
+      if (int rc = rwt::learned_sort_enqueue(b->learned, keys + p0, alt + p0, nc, b->learned_mode,
+                                             b->learned_fallback, true, s))
+        return rc;
+    }
+  }
+  if (!b->learned) RWB_CUDA(rwt::launch_keys(x, sc, pl, true, true, s));
   const size_t radix = size_t(1) << b->radix_bits;
-  for (uint32_t k = 0; k < b->n_classes; ++k) {
+  for (uint32_t k = 0; k < b->n_classes && !b->learned; ++k) {
     if (!b->class_tiles[k]) continue;
     rwt::Scratch sk = sc;
     sk.sort_variant = b->class_variant[k];

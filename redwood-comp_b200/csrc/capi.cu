@@ -158,11 +158,14 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 int sort_enqueue_gated(rw_tree_im_storage* im, const void* keys, void* out, uint32_t n,
                        const uint32_t* gate, bool clear, cudaStream_t s) {
+  // internal callers pass key ranges of a batch, which start anywhere: the
+  // sort's kernels load and store keys one at a time, so only the word
+  // alignment of the key type is needed
+  if (!im || !keys || !out || n < 1 || n > im->n_cap || n >= RW_MAX_POINTS) return RW_ERR_ARG;
   rw_tree_app_data app;
-  rw_tree_app_data_init(&app, n, im ? im->key_bits : 32);
+  rw_tree_app_data_init(&app, n, im->key_bits);
   app.u_morton_keys = const_cast<void*>(keys);
   app.u_morton_keys_alt = out;
-  if (int rc = check(&app, im, kKeys | kAlt)) return rc;
   if (clear)
     if (int rc = clear_all(im, s)) return rc;
   const auto b = bufs_of(app, im);

@@ -176,6 +176,7 @@ int learned_sort_enqueue(rw_tree_learned* L, const uint32_t* keys, uint32_t* sor
                          int32_t mode, rw_tree_im_storage* fallback_im, bool clear_fallback,
                          cudaStream_t s);
 void learned_last_stats(const rw_tree_learned* L, rw_tree_learned_stats* out);
+uint32_t learned_capacity(const rw_tree_learned* L);  // n_max it was created for
 
 // Test hook of the bounded look-back wait: the digit histograms of b.keys,
 // then pass 0 of the sort into b.alt with tile 0 left out, so that every

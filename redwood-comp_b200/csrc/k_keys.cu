@@ -168,7 +168,10 @@ struct BinCfg {
   static constexpr int TILE = THREADS * KPT;
   static constexpr size_t kKeysBytes = size_t(TILE) * sizeof(K);
   static constexpr size_t kHistBytes = size_t(NW) * RADIX * 4;
-  static constexpr size_t kMatchBytes = RANK == kRankAtomicOr ? kHistBytes : 0;
+  // the two-array scheme keeps a match-mask array beside the counters; the
+  // half-warp scheme has two words per digit and warp (one per half-warp)
+  static constexpr size_t kMatchBytes =
+      (RANK == kRankAtomicOr || RANK == kRankHalfPacked) ? kHistBytes : 0;
   static constexpr size_t kSmem =
       kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
   static_assert(kSmem <= 227 * 1024, "onesweep variant exceeds shared memory per CTA");
@@ -202,7 +205,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
   {
     static_assert((NW * RADIX) % 4 == 0 && C::kKeysBytes % 16 == 0, "16-byte zeroing");
     const uint4 z = make_uint4(0, 0, 0, 0);
-    constexpr int kWords = (RANK == kRankAtomicOr ? 2 : 1) * NW * RADIX;  // s_hist, s_match
+    constexpr int kWords =
+        (RANK == kRankAtomicOr || RANK == kRankHalfPacked ? 2 : 1) * NW * RADIX;
     for (int i = tid; i < kWords / 4; i += THREADS) reinterpret_cast<uint4*>(s_hist)[i] = z;
   }
   __syncthreads();
@@ -216,12 +220,29 @@ __global__ void __launch_bounds__(THREADS, MINB)
   const bool full = base + TILE <= n;
 
   // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
+  // (half-warp scheme: half h of warp w owns [w*32*KPT + h*16*KPT, +16*KPT),
+  // 16 keys per step)
   K keys[KPT];
   uint32_t rank2[RankPack<KPT>::kRegs];  // packed warp ranks
   const uint32_t wbase = base + warp * 32u * KPT + lane;
+  const uint32_t hbase = base + warp * 32u * KPT + (lane >> 4) * 16u * KPT + (lane & 15u);
   uint32_t* wh = s_hist + warp * RADIX;
   uint32_t* wm = s_match + warp * RADIX;
-  if (full) {
+  uint32_t* wp = s_hist + warp * 2u * RADIX;  // half-warp scheme: [2 RADIX] per warp
+  if (RANK == kRankHalfPacked) {
+    if (full) {
+#pragma unroll
+      for (int i = 0; i < KPT; ++i) keys[i] = in[hbase + 16u * i];
+      half_rank<D, KPT, true>(keys, rank2, shift, hbase, n, wp);
+    } else {
+#pragma unroll
+      for (int i = 0; i < KPT; ++i) {
+        const uint32_t idx = hbase + 16u * i;
+        keys[i] = idx < n ? in[idx] : K(0);
+      }
+      half_rank<D, KPT, false>(keys, rank2, shift, hbase, n, wp);
+    }
+  } else if (full) {
 #pragma unroll
     for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
     warp_rank<D, KPT, RANK, true>(keys, rank2, shift, wbase, n, wh, wm);
@@ -235,32 +256,67 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
   __syncthreads();
 
-  // per digit: exclusive scan over warps and publish the tile aggregate
+  // per digit: exclusive scan over warps (half-warps) and publish the tile
+  // aggregate
   uint32_t* drow = desc + size_t(row) * RADIX;
-  for (int d = tid; d < RADIX; d += THREADS) {
-    uint32_t run = 0;
+  if (RANK == kRankHalfPacked) {
+    // lane pairs own a digit: the even lane its half-warp-0 words, the odd
+    // lane its half-warp-1 words (consecutive addresses, no bank conflicts);
+    // units run in the order (warp, half), the partner's count by a shuffle
+    static_assert((2 * RADIX) % 32 == 0 && THREADS % 32 == 0, "whole warps per pass");
+    for (int x = tid; x < 2 * RADIX; x += THREADS) {
+      const uint32_t h = uint32_t(x) & 1u;
+      uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < NW; ++w) {
-      const uint32_t c = s_hist[w * RADIX + d];
-      s_hist[w * RADIX + d] = run;
-      run += c;
+      for (int w = 0; w < NW; ++w) {
+        uint32_t* p = s_hist + w * 2 * RADIX + x;
+        const uint32_t mine = *p >> 16;
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, 1);
+        *p = run + (h ? other : 0u);
+        run += mine + other;
+      }
+      if (!h) {
+        s_cnt[x >> 1] = run;
+        st_relaxed(drow + (x >> 1), kFlagAgg | (run << 2));
+      }
     }
-    s_cnt[d] = run;
-    st_relaxed(drow + d, kFlagAgg | (run << 2));
+  } else {
+    for (int d = tid; d < RADIX; d += THREADS) {
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const uint32_t c = s_hist[w * RADIX + d];
+        s_hist[w * RADIX + d] = run;
+        run += c;
+      }
+      s_cnt[d] = run;
+      st_relaxed(drow + d, kFlagAgg | (run << 2));
+    }
   }
   __syncthreads();
   digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
   __syncthreads();
   // fold the digit starts into the per-warp offsets once per tile, so that
   // placing a key below reads one shared-memory word instead of two
-  for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] += s_start[i & (RADIX - 1)];
+  if (RANK == kRankHalfPacked) {
+    for (int i = tid; i < 2 * NW * RADIX; i += THREADS)
+      s_hist[i] += s_start[(i >> 1) & (RADIX - 1)];
+  } else {
+    for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] += s_start[i & (RADIX - 1)];
+  }
   __syncthreads();
 
   // reorder the tile by digit in shared memory first: it needs only the
   // tile's own counts, and gives the predecessors time to publish their
   // inclusive prefixes before the look-back below reads them
-  if (full) warp_place<D, KPT, true>(keys, rank2, shift, wbase, n, wh, s_keys);
-  else warp_place<D, KPT, false>(keys, rank2, shift, wbase, n, wh, s_keys);
+  if (RANK == kRankHalfPacked) {
+    if (full) half_place<D, KPT, true>(keys, rank2, shift, hbase, n, wp, s_keys);
+    else half_place<D, KPT, false>(keys, rank2, shift, hbase, n, wp, s_keys);
+  } else if (full) {
+    warp_place<D, KPT, true>(keys, rank2, shift, wbase, n, wh, s_keys);
+  } else {
+    warp_place<D, KPT, false>(keys, rank2, shift, wbase, n, wh, s_keys);
+  }
 
   // decoupled look-back, kLookback descriptors per round trip.  The segment's
   // first row is always inclusive, so rows are read clamped to it and the
@@ -413,6 +469,10 @@ struct SortVariant {
 // the default).
 const SortVariant kVariants[] = {
     {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 3>},
+    {32, 8, 384, 24, kRankHalfPacked, passes_t<uint32_t, 8, 384, 24, kRankHalfPacked, 3>},
+    {32, 8, 512, 16, kRankHalfPacked, passes_t<uint32_t, 8, 512, 16, kRankHalfPacked, 2>},
+    {32, 8, 256, 24, kRankHalfPacked, passes_t<uint32_t, 8, 256, 24, kRankHalfPacked, 4>},
+    {32, 8, 512, 24, kRankHalfPacked, passes_t<uint32_t, 8, 512, 24, kRankHalfPacked, 2>},
     {32, 8, 512, 16, kRankAtomicOr, passes_t<uint32_t, 8, 512, 16, kRankAtomicOr, 2>},
     {32, 8, 384, 16, kRankAtomicOr, passes_t<uint32_t, 8, 384, 16, kRankAtomicOr, 2>},
     {32, 8, 256, 16, kRankAtomicOr, passes_t<uint32_t, 8, 256, 16, kRankAtomicOr, 3>},
@@ -434,6 +494,8 @@ const SortVariant kVariants[] = {
     {32, 11, 256, 16, kRankBallot, passes_t<uint32_t, 11, 256, 16, kRankBallot, 2>},
     {32, 11, 384, 16, kRankBallot, passes_t<uint32_t, 11, 384, 16, kRankBallot, 1>},
     {64, 8, 384, 16, kRankAtomicOr, passes_t<uint64_t, 8, 384, 16, kRankAtomicOr, 2>},
+    {64, 8, 384, 16, kRankHalfPacked, passes_t<uint64_t, 8, 384, 16, kRankHalfPacked, 2>},
+    {64, 8, 256, 16, kRankHalfPacked, passes_t<uint64_t, 8, 256, 16, kRankHalfPacked, 3>},
     {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},
     {64, 8, 256, 12, kRankAtomicOr, passes_t<uint64_t, 8, 256, 12, kRankAtomicOr, 3>},
     {64, 8, 256, 16, kRankBallot, passes_t<uint64_t, 8, 256, 16, kRankBallot, 2>},

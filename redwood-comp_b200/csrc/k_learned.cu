@@ -336,7 +336,9 @@ __global__ void __launch_bounds__(kSpThreads, 2)
   for (uint32_t i = threadIdx.x; i < BINS; i += kSpThreads) s_cnt[i] = 0;
   __syncthreads();
   uint32_t k[kSpKpt];
-  const bool full = tile_n == kSpTile;
+  // vector loads need a whole tile on a 16-byte boundary (a cloud of a batch
+  // may start anywhere)
+  const bool full = tile_n == kSpTile && (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
   if (full) {
     const uint4* v = reinterpret_cast<const uint4*>(in);
 #pragma unroll
@@ -850,6 +852,8 @@ int learned_sort_enqueue(rw_tree_learned* L, const uint32_t* keys, uint32_t* sor
   RWL_CUDA(cudaGetLastError());
   return sort_enqueue_gated(fallback_im, keys, sorted, n, &L->d_plan->fallback, clear_fallback, s);
 }
+
+uint32_t learned_capacity(const rw_tree_learned* L) { return L ? L->n_max : 0u; }
 
 void learned_last_stats(const rw_tree_learned* L, rw_tree_learned_stats* out) {
   std::memset(out, 0, sizeof *out);

@@ -35,7 +35,12 @@ __device__ __forceinline__ void digit_exclusive_scan(const uint32_t* s_cnt,
 // Warp ranking schemes: all return, for each lane, the mask of valid lanes in
 // its warp holding the same digit (the lane's stable rank is the popcount of
 // the mask below it).
-enum RankMode : int { kRankBallot = 0, kRankMatchAny = 1, kRankAtomicOr = 2 };
+enum RankMode : int {
+  kRankBallot = 0,
+  kRankMatchAny = 1,
+  kRankAtomicOr = 2,
+  kRankHalfPacked = 3  // per half-warp: one word per digit, count << 16 | 16-lane mask
+};
 
 // D ballots, one per digit bit (warp-level multi-split).
 template <int D>
@@ -121,6 +126,62 @@ __device__ __forceinline__ void warp_place(const K (&keys)[KPT],
     if (FULL || wbase + 32u * i < n) {
       const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
       s_keys[wh[dig] + RankPack<KPT>::get(rank2, i)] = keys[i];
+    }
+  }
+}
+
+// ---- half-warp packed ranking (kRankHalfPacked) -----------------------------
+// Each half-warp (16 lanes) owns a contiguous run of 16 * KPT keys of its
+// warp's 32 * KPT (key i of lane l at position 16 i + (l & 15) of the run), so
+// ranks in the order (half-warp, step, lane) are stable.  Per digit a half-warp
+// has one shared-memory word: the count of its earlier keys of that digit in
+// the high 16 bits and, during a step, the mask of its lanes holding the digit
+// in the low 16 bits.  A step costs an atomic OR, one read of the word (count
+// and peers together, no shuffle) and the leader's store of the new count -
+// three shared-memory accesses where the two-array scheme needs four.  The
+// words of half-warp h of a warp sit at 2 d + h: the two halves use the even
+// and the odd banks, so their accesses never conflict with each other.
+__device__ __forceinline__ uint32_t half_slot(uint32_t dig) {
+  return 2u * dig + (lane_id() >> 4);
+}
+
+template <int D, int KPT, bool FULL, typename K>
+__device__ __forceinline__ void half_rank(const K (&keys)[KPT],
+                                          uint32_t (&rank2)[RankPack<KPT>::kRegs], int shift,
+                                          uint32_t hbase, uint32_t n, uint32_t* wp) {
+  constexpr uint32_t RADIX = 1u << D;
+  const uint32_t l16 = lane_id() & 15u;
+  const uint32_t lt16 = (1u << l16) - 1u;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const bool valid = FULL || hbase + 16u * i < n;
+    const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
+    uint32_t* w = wp + half_slot(dig);
+    if (valid) atomicOr(w, 1u << l16);
+    __syncwarp();
+    const uint32_t word = valid ? *w : 0u;
+    const uint32_t peers = word & 0xffffu, cnt = word >> 16;
+    const uint32_t below = __popc(peers & lt16);
+    __syncwarp();
+    if (valid && below == 0) *w = (cnt + uint32_t(__popc(peers))) << 16;
+    RankPack<KPT>::set(rank2, i, cnt + below);
+    __syncwarp();
+  }
+}
+
+// Places the half-warp's keys at their tile positions (wp: the warp's
+// per-half-warp offsets, laid out as half_slot says).
+template <int D, int KPT, bool FULL, typename K>
+__device__ __forceinline__ void half_place(const K (&keys)[KPT],
+                                           const uint32_t (&rank2)[RankPack<KPT>::kRegs],
+                                           int shift, uint32_t hbase, uint32_t n,
+                                           const uint32_t* wp, K* s_keys) {
+  constexpr uint32_t RADIX = 1u << D;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    if (FULL || hbase + 16u * i < n) {
+      const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
+      s_keys[wp[half_slot(dig)] + RankPack<KPT>::get(rank2, i)] = keys[i];
     }
   }
 }

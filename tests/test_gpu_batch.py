@@ -100,3 +100,34 @@ def test_batch_size_classes(rw, oracle):
     batch.set_classes([(4000, v32[2]), (30000, v32[1]), (1 << 30, v32[0])])
     batch.run(graph=True)
     assert check_batch(rw, oracle, batch, clouds, 32)["ok"] == len(clouds)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_with_learned_sort_every_cloud_exact(rw, oracle, mode):
+    """Stage 2 of every cloud by the learned-CDF sort inside the batch (the
+    combined form): clouds above and below the 65,536-key sample, starting at
+    offsets that are not 16-byte aligned, one of them with a dense spot that
+    overflows its bucket region (the gated onesweep fallback), through the
+    CUDA graph and without it - every cloud equals the oracle's run on it."""
+    from redwood_comp_b200 import learned
+    clouds = [learned.mixture_cloud(rw, 200_003, 41_001),
+              rw.generate_points(1_001, rw.GEN_UNIFORM, 41_002),
+              rw.generate_points(150_001, rw.GEN_UNIFORM, 41_003),
+              learned.mixture_cloud(rw, 65_537, 41_004),
+              rw.generate_points(120_000, rw.GEN_UNIFORM, 41_005)]
+    clouds[4][:30_000] = np.float32(700.5)  # a quarter of the cloud on one spot
+    largest = max(c.shape[0] for c in clouds)
+    L = rw.Learned(largest)
+    if L.params is None:
+        L.set_params(learned.init_params(1))
+    fallback = rw.ImStorage(largest, 32)
+    batch = rw.Batch(clouds, 32, octree_ratio=1.0)
+    batch.set_learned(L, mode, fallback)
+    for graph in (False, True, True):
+        batch.run(graph=graph)
+        counted = check_batch(rw, oracle, batch, clouds, 32)
+        assert counted["ok"] == len(clouds), counted
+    batch.set_learned(None)
+    batch.run(graph=True)
+    assert check_batch(rw, oracle, batch, clouds, 32)["ok"] == len(clouds)
+    batch.close()
