@@ -345,11 +345,14 @@ def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
 
 
 def measure_combined(rw, a, n_clouds=64, lo=1 << 20, hi=8 << 20, seed=880_001):
-    """The batched pipeline on 64 large clouds (sizes log-uniform in [1M, 8M],
-    Gaussian mixtures with 8-64 components, 64-bit keys) against the plain
-    pipeline run once per cloud; every cloud's outputs compared on the device
-    with its plain run.  (Stage 2 here is the onesweep sort: the learned-CDF
-    sort serves 32-bit keys.)"""
+    """The combined configuration: 64 clouds, sizes log-uniform in [1M, 8M],
+    Gaussian mixtures with 8-64 components, through the batched pipeline
+    against the plain pipeline run once per cloud, every cloud's outputs
+    compared on the device with its plain run.  64-bit keys with the batched
+    onesweep sort; then the same clouds with 32-bit keys, the batched pipeline
+    with the learned-CDF sort (MLP boundaries) as stage 2 of every cloud
+    against the batched onesweep and the plain per-cloud runs (the learned
+    sort serves 32-bit keys)."""
     import torch
     rng = np.random.default_rng(seed)
     sizes = [int(np.exp(rng.uniform(np.log(lo), np.log(hi)))) for _ in range(n_clouds)]
@@ -359,67 +362,98 @@ def measure_combined(rw, a, n_clouds=64, lo=1 << 20, hi=8 << 20, seed=880_001):
               for c, nc in enumerate(sizes)]
     total = int(sum(sizes))
     ratio = 1.0
-    batch = rw.Batch(clouds, 64, octree_ratio=ratio)
     s = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for _ in range(3):
-        batch.run(graph=True)
-    torch.cuda.synchronize()
     reps = 3
-    e0.record(s)
-    for _ in range(reps):
-        batch.enqueue(graph=True)
-    e1.record(s)
-    batch.finish()
-    batch_ms = e0.elapsed_time(e1) / reps
-    failed = int((batch.status != 0).sum())
-    # plain: one AppData/scratch per cloud, launches back to back
-    im = rw.ImStorage(max(sizes), 64)
-    apps = [rw.AppData(nc, 64, points=cl, octree_ratio=ratio) for nc, cl in zip(sizes, clouds)]
-    del clouds
 
-    def plain_once():
-        for app in apps:
-            rw.pipeline_enqueue(app, im)
-        rw.pipeline_finish(apps[-1], im)
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
 
-    plain_once()
-    torch.cuda.synchronize()
-    e0.record(s)
-    for _ in range(reps):
-        plain_once()
-    e1.record(s)
-    torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / reps
-    mism = 0
-    for c, app in enumerate(apps):  # every cloud against its own plain run
-        rw.run_pipeline(app, im)
-        p0 = int(batch.point_offsets[c])
-        r0 = int(batch.octree_offsets[c])
-        u, m = app.get_n_unique(), app.get_n_octree_nodes()
-        same = int(batch.n_unique[c]) == u and int(batch.n_octree_nodes[c]) == m
-        pairs = [(batch.morton_keys_alt[p0:p0 + app.n_input], app.u_morton_keys_alt),
-                 (batch.morton_keys[p0:p0 + u], app.u_morton_keys[:u])]
-        for bf, af in (("prefix_n", "brt_prefix_n"), ("has_leaf_left", "brt_has_leaf_left"),
-                       ("has_leaf_right", "brt_has_leaf_right"), ("left_child", "brt_left_child"),
-                       ("parents", "brt_parents"), ("edge_count", "u_edge_count"),
-                       ("edge_offset", "u_edge_offset")):
-            pairs.append((getattr(batch, bf)[p0:p0 + u - 1], getattr(app, af)[:u - 1]))
-        for bf, af in (("children", "oct_children"), ("corner", "oct_corner"),
-                       ("cell_size", "oct_cell_size"), ("child_node_mask", "oct_child_node_mask"),
-                       ("child_leaf_mask", "oct_child_leaf_mask")):
-            pairs.append((getattr(batch, bf)[r0:r0 + m], getattr(app, af)[:m]))
-        mism += int(not same or not all(torch.equal(x, y) for x, y in pairs))
+    def compare(batch, apps, im):
+        mism = 0
+        for c, app in enumerate(apps):  # every cloud against its own plain run
+            rw.run_pipeline(app, im)
+            p0 = int(batch.point_offsets[c])
+            r0 = int(batch.octree_offsets[c])
+            u, m = app.get_n_unique(), app.get_n_octree_nodes()
+            same = int(batch.n_unique[c]) == u and int(batch.n_octree_nodes[c]) == m
+            pairs = [(batch.morton_keys_alt[p0:p0 + app.n_input], app.u_morton_keys_alt),
+                     (batch.morton_keys[p0:p0 + u], app.u_morton_keys[:u])]
+            for bf, af in (("prefix_n", "brt_prefix_n"), ("has_leaf_left", "brt_has_leaf_left"),
+                           ("has_leaf_right", "brt_has_leaf_right"),
+                           ("left_child", "brt_left_child"), ("parents", "brt_parents"),
+                           ("edge_count", "u_edge_count"), ("edge_offset", "u_edge_offset")):
+                pairs.append((getattr(batch, bf)[p0:p0 + u - 1], getattr(app, af)[:u - 1]))
+            for bf, af in (("children", "oct_children"), ("corner", "oct_corner"),
+                           ("cell_size", "oct_cell_size"),
+                           ("child_node_mask", "oct_child_node_mask"),
+                           ("child_leaf_mask", "oct_child_leaf_mask")):
+                pairs.append((getattr(batch, bf)[r0:r0 + m], getattr(app, af)[:m]))
+            mism += int(not same or not all(torch.equal(x, y) for x, y in pairs))
+        return mism
+
+    def run_width(key_bits, learned_too):
+        batch = rw.Batch(clouds, key_bits, octree_ratio=ratio)
+        out = {}
+        batch_ms = timed(lambda: batch.run(graph=True))
+        failed = int((batch.status != 0).sum())
+        im = rw.ImStorage(max(sizes), key_bits)
+        apps = [rw.AppData(nc, key_bits, points=cl, octree_ratio=ratio)
+                for nc, cl in zip(sizes, clouds)]
+
+        def plain_once():
+            for app in apps:
+                rw.pipeline_enqueue(app, im)
+            rw.pipeline_finish(apps[-1], im)
+
+        plain_ms = timed(plain_once)
+        out["onesweep"] = {"value": total / (batch_ms / 1e3), "ms_per_batch": batch_ms,
+                           "speedup_vs_plain": plain_ms / batch_ms, "clouds_failed": failed,
+                           "mismatched_clouds": compare(batch, apps, im)}
+        if learned_too:
+            L = rw.Learned(max(sizes))
+            fb = rw.ImStorage(max(sizes), key_bits)
+            if L.params is not None:
+                batch.set_learned(L, rw.LEARNED_MLP, fb)
+                lms = timed(lambda: batch.run(graph=True))
+                out["learned_mlp"] = {
+                    "value": total / (lms / 1e3), "ms_per_batch": lms,
+                    "speedup_vs_plain": plain_ms / lms, "speedup_vs_batched_onesweep":
+                        batch_ms / lms, "clouds_failed": int((batch.status != 0).sum()),
+                    "mismatched_clouds": compare(batch, apps, im)}
+                batch.set_learned(None)
+            L.close()
+        out["plain_per_cloud_value"] = total / (plain_ms / 1e3)
+        out["plain_per_cloud_ms"] = plain_ms
+        batch.close()
+        del apps, im
+        torch.cuda.empty_cache()
+        return out
+
+    w64 = run_width(64, False)
+    w32 = run_width(32, True)
     info = {
         "workload": f"combined: {n_clouds} clouds, sizes log-uniform in [1M, 8M] (total "
-                    f"{total:,} points), Gaussian mixtures with 8-64 components, 64-bit keys, "
-                    f"octree rows {ratio} per point; stage 2 onesweep (no 64-bit learned sort)",
-        "value": total / (batch_ms / 1e3), "unit": "points/s", "ms_per_batch": batch_ms,
-        "plain_per_cloud_value": total / (plain_ms / 1e3), "plain_per_cloud_ms": plain_ms,
-        "speedup_vs_plain": plain_ms / batch_ms, "clouds_failed": failed,
-        "clouds_compared_with_plain": n_clouds, "mismatched_clouds": mism, "graph": True,
+                    f"{total:,} points), Gaussian mixtures with 8-64 components, octree rows "
+                    f"{ratio} per point",
+        "unit": "points/s", "graph": True,
+        # the 64-bit line (BASELINE's key width for this configuration)
+        "value": w64["onesweep"]["value"], "ms_per_batch": w64["onesweep"]["ms_per_batch"],
+        "plain_per_cloud_value": w64["plain_per_cloud_value"],
+        "plain_per_cloud_ms": w64["plain_per_cloud_ms"],
+        "speedup_vs_plain": w64["onesweep"]["speedup_vs_plain"],
+        "clouds_failed": w64["onesweep"]["clouds_failed"],
+        "clouds_compared_with_plain": n_clouds,
+        "mismatched_clouds": w64["onesweep"]["mismatched_clouds"],
+        "key_bits_64": w64, "key_bits_32": w32,
     }
-    batch.close()
     return info
 
 
