@@ -36,6 +36,8 @@
 #include <cstdint>
 #include <cstring>
 #include <memory_resource>
+#include <stdexcept>
+#include <string>
 
 #include "app_data.hpp"
 #include "cuda/cu_dispatcher.cuh"
@@ -90,6 +92,15 @@ __global__ void k_check_increasing(const unsigned* __restrict__ keys, int n,
     if (keys[i - 1] >= keys[i]) atomicAdd(flags, 1u);
 }
 
+// A launch error of a reference stage (its dispatcher checks only the stream
+// synchronisation) is reported with the stage's number.
+void stage_done(int k) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw std::runtime_error("reference stage " + std::to_string(k) + ": " +
+                             cudaGetErrorString(e));
+}
+
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
       .count();
@@ -137,11 +148,14 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
       for (int it = 0; it < iters; ++it) {
         auto t0 = std::chrono::steady_clock::now();
         cuda::run_stage1(app, stream);
+        stage_done(1);
         cuda::run_stage2(app, im, stream);
+        stage_done(2);
         CUDA_CHECK(cudaMemcpyAsync(app.u_morton_keys_alt.data(), app.u_morton_keys.data(),
                                    size_t(4) * n, cudaMemcpyDeviceToDevice, stream));
         CUDA_CHECK(cudaStreamSynchronize(stream));
         cuda::run_stage3(app, im, stream);
+        stage_done(3);
         double ms = ms_since(t0);
         const int nu = static_cast<int>(app.get_n_unique());
         const bool sorted = nu >= 3 && nu <= static_cast<int>(n) && check([&] {
@@ -155,8 +169,11 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
         }
         t0 = std::chrono::steady_clock::now();
         cuda::run_stage4(app, stream);
+        stage_done(4);
         cuda::run_stage5(app, stream);
+        stage_done(5);
         cuda::run_stage6(app, stream);
+        stage_done(6);
         ms += ms_since(t0);
         last_m = app.get_n_octree_nodes();
         const bool rows_ok = check([&] {
@@ -167,6 +184,7 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
         if (rows_ok) {
           t0 = std::chrono::steady_clock::now();
           cuda::run_stage7(app, stream);
+          stage_done(7);
           ms += ms_since(t0);
         } else {
           all_ran = false;

@@ -180,7 +180,12 @@ struct BinCfg {
 // One onesweep pass over `n` keys: digit `shift`..`shift+D-1`, stable.
 // desc: [(tiles + 1) x RADIX] descriptors, row 0 prefilled with the global
 // exclusive digit offsets (k_sort_init), rows 1.. zero.
-template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
+// PERSIST: a CTA takes tiles by ticket until they run out (a grid of at most
+// one wave), instead of one tile per CTA.  Used when the pass is gated, so
+// that a pass that is not needed costs one short wave of CTAs.  A CTA holds a
+// ticket only while it runs, so every look-back still waits only on running
+// tiles, whatever the grid.
+template <typename K, int D, int THREADS, int KPT, int RANK, int MINB, bool PERSIST>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
@@ -201,180 +206,185 @@ __global__ void __launch_bounds__(THREADS, MINB)
   uint32_t* s_misc = s_gofs + RADIX;  // [0] tile, [1..] warp scan scratch
 
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  if (tid == 0) s_misc[0] = atomicAdd(tile_ctr, 1u);
-  {
-    static_assert((NW * RADIX) % 4 == 0 && C::kKeysBytes % 16 == 0, "16-byte zeroing");
-    const uint4 z = make_uint4(0, 0, 0, 0);
-    constexpr int kWords =
-        (RANK == kRankAtomicOr || RANK == kRankHalfPacked ? 2 : 1) * NW * RADIX;
-    for (int i = tid; i < kWords / 4; i += THREADS) reinterpret_cast<uint4*>(s_hist)[i] = z;
-  }
-  __syncthreads();
-  const uint32_t tile = s_misc[0];
-  uint32_t first_tile;
-  const uint32_t segc = tile_segment(seg, map, tile, &first_tile);
-  const uint32_t base = seg_begin(seg, segc) + (tile - first_tile) * TILE;
-  const uint32_t n = seg_begin(seg, segc) + seg_size(seg, segc);  // end of the segment
-  const int row = int(tile + segc + 1);       // this tile's descriptor row
-  const int init_row = int(first_tile + segc);  // the segment's inclusive row
-  const bool full = base + TILE <= n;
+  for (;;) {
+    if (tid == 0) s_misc[0] = atomicAdd(tile_ctr, 1u);
+    {
+      static_assert((NW * RADIX) % 4 == 0 && C::kKeysBytes % 16 == 0, "16-byte zeroing");
+      const uint4 z = make_uint4(0, 0, 0, 0);
+      constexpr int kWords =
+          (RANK == kRankAtomicOr || RANK == kRankHalfPacked ? 2 : 1) * NW * RADIX;
+      for (int i = tid; i < kWords / 4; i += THREADS) reinterpret_cast<uint4*>(s_hist)[i] = z;
+    }
+    __syncthreads();
+    const uint32_t tile = s_misc[0];
+    if (PERSIST && tile >= map.n_tiles) break;  // block-uniform
+    uint32_t first_tile;
+    const uint32_t segc = tile_segment(seg, map, tile, &first_tile);
+    const uint32_t base = seg_begin(seg, segc) + (tile - first_tile) * TILE;
+    const uint32_t n = seg_begin(seg, segc) + seg_size(seg, segc);  // end of the segment
+    const int row = int(tile + segc + 1);       // this tile's descriptor row
+    const int init_row = int(first_tile + segc);  // the segment's inclusive row
+    const bool full = base + TILE <= n;
 
-  // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
-  // (half-warp scheme: half h of warp w owns [w*32*KPT + h*16*KPT, +16*KPT),
-  // 16 keys per step)
-  K keys[KPT];
-  uint32_t rank2[RankPack<KPT>::kRegs];  // packed warp ranks
-  const uint32_t wbase = base + warp * 32u * KPT + lane;
-  const uint32_t hbase = base + warp * 32u * KPT + (lane >> 4) * 16u * KPT + (lane & 15u);
-  uint32_t* wh = s_hist + warp * RADIX;
-  uint32_t* wm = s_match + warp * RADIX;
-  uint32_t* wp = s_hist + warp * 2u * RADIX;  // half-warp scheme: [2 RADIX] per warp
-  if (RANK == kRankHalfPacked) {
-    if (full) {
-#pragma unroll
-      for (int i = 0; i < KPT; ++i) keys[i] = in[hbase + 16u * i];
-      half_rank<D, KPT, true>(keys, rank2, shift, hbase, n, wp);
+    // load: warp w owns [w*32*KPT, (w+1)*32*KPT) of the tile, 32 keys per step
+    // (half-warp scheme: half h of warp w owns [w*32*KPT + h*16*KPT, +16*KPT),
+    // 16 keys per step)
+    K keys[KPT];
+    uint32_t rank2[RankPack<KPT>::kRegs];  // packed warp ranks
+    const uint32_t wbase = base + warp * 32u * KPT + lane;
+    const uint32_t hbase = base + warp * 32u * KPT + (lane >> 4) * 16u * KPT + (lane & 15u);
+    uint32_t* wh = s_hist + warp * RADIX;
+    uint32_t* wm = s_match + warp * RADIX;
+    uint32_t* wp = s_hist + warp * 2u * RADIX;  // half-warp scheme: [2 RADIX] per warp
+    if (RANK == kRankHalfPacked) {
+      if (full) {
+  #pragma unroll
+        for (int i = 0; i < KPT; ++i) keys[i] = in[hbase + 16u * i];
+        half_rank<D, KPT, true>(keys, rank2, shift, hbase, n, wp);
+      } else {
+  #pragma unroll
+        for (int i = 0; i < KPT; ++i) {
+          const uint32_t idx = hbase + 16u * i;
+          keys[i] = idx < n ? in[idx] : K(0);
+        }
+        half_rank<D, KPT, false>(keys, rank2, shift, hbase, n, wp);
+      }
+    } else if (full) {
+  #pragma unroll
+      for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
+      warp_rank<D, KPT, RANK, true>(keys, rank2, shift, wbase, n, wh, wm);
     } else {
-#pragma unroll
+  #pragma unroll
       for (int i = 0; i < KPT; ++i) {
-        const uint32_t idx = hbase + 16u * i;
+        const uint32_t idx = wbase + 32u * i;
         keys[i] = idx < n ? in[idx] : K(0);
       }
-      half_rank<D, KPT, false>(keys, rank2, shift, hbase, n, wp);
+      warp_rank<D, KPT, RANK, false>(keys, rank2, shift, wbase, n, wh, wm);
     }
-  } else if (full) {
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
-    warp_rank<D, KPT, RANK, true>(keys, rank2, shift, wbase, n, wh, wm);
-  } else {
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      const uint32_t idx = wbase + 32u * i;
-      keys[i] = idx < n ? in[idx] : K(0);
-    }
-    warp_rank<D, KPT, RANK, false>(keys, rank2, shift, wbase, n, wh, wm);
-  }
-  __syncthreads();
+    __syncthreads();
 
-  // per digit: exclusive scan over warps (half-warps) and publish the tile
-  // aggregate
-  uint32_t* drow = desc + size_t(row) * RADIX;
-  if (RANK == kRankHalfPacked) {
-    // lane pairs own a digit: the even lane its half-warp-0 words, the odd
-    // lane its half-warp-1 words (consecutive addresses, no bank conflicts);
-    // units run in the order (warp, half), the partner's count by a shuffle
-    static_assert((2 * RADIX) % 32 == 0 && THREADS % 32 == 0, "whole warps per pass");
-    for (int x = tid; x < 2 * RADIX; x += THREADS) {
-      const uint32_t h = uint32_t(x) & 1u;
-      uint32_t run = 0;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        uint32_t* p = s_hist + w * 2 * RADIX + x;
-        const uint32_t mine = *p >> 16;
-        const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, 1);
-        *p = run + (h ? other : 0u);
-        run += mine + other;
+    // per digit: exclusive scan over warps (half-warps) and publish the tile
+    // aggregate
+    uint32_t* drow = desc + size_t(row) * RADIX;
+    if (RANK == kRankHalfPacked) {
+      // lane pairs own a digit: the even lane its half-warp-0 words, the odd
+      // lane its half-warp-1 words (consecutive addresses, no bank conflicts);
+      // units run in the order (warp, half), the partner's count by a shuffle
+      static_assert((2 * RADIX) % 32 == 0 && THREADS % 32 == 0, "whole warps per pass");
+      for (int x = tid; x < 2 * RADIX; x += THREADS) {
+        const uint32_t h = uint32_t(x) & 1u;
+        uint32_t run = 0;
+  #pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          uint32_t* p = s_hist + w * 2 * RADIX + x;
+          const uint32_t mine = *p >> 16;
+          const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, 1);
+          *p = run + (h ? other : 0u);
+          run += mine + other;
+        }
+        if (!h) {
+          s_cnt[x >> 1] = run;
+          st_relaxed(drow + (x >> 1), kFlagAgg | (run << 2));
+        }
       }
-      if (!h) {
-        s_cnt[x >> 1] = run;
-        st_relaxed(drow + (x >> 1), kFlagAgg | (run << 2));
+    } else {
+      for (int d = tid; d < RADIX; d += THREADS) {
+        uint32_t run = 0;
+  #pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          const uint32_t c = s_hist[w * RADIX + d];
+          s_hist[w * RADIX + d] = run;
+          run += c;
+        }
+        s_cnt[d] = run;
+        st_relaxed(drow + d, kFlagAgg | (run << 2));
       }
     }
-  } else {
+    __syncthreads();
+    digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
+    __syncthreads();
+    // fold the digit starts into the per-warp offsets once per tile, so that
+    // placing a key below reads one shared-memory word instead of two
+    if (RANK == kRankHalfPacked) {
+      for (int i = tid; i < 2 * NW * RADIX; i += THREADS)
+        s_hist[i] += s_start[(i >> 1) & (RADIX - 1)];
+    } else {
+      for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] += s_start[i & (RADIX - 1)];
+    }
+    __syncthreads();
+
+    // reorder the tile by digit in shared memory first: it needs only the
+    // tile's own counts, and gives the predecessors time to publish their
+    // inclusive prefixes before the look-back below reads them
+    if (RANK == kRankHalfPacked) {
+      if (full) half_place<D, KPT, true>(keys, rank2, shift, hbase, n, wp, s_keys);
+      else half_place<D, KPT, false>(keys, rank2, shift, hbase, n, wp, s_keys);
+    } else if (full) {
+      warp_place<D, KPT, true>(keys, rank2, shift, wbase, n, wh, s_keys);
+    } else {
+      warp_place<D, KPT, false>(keys, rank2, shift, wbase, n, wh, s_keys);
+    }
+
+    // decoupled look-back, kLookback descriptors per round trip.  The segment's
+    // first row is always inclusive, so rows are read clamped to it and the
+    // walk stops there at the latest.
     for (int d = tid; d < RADIX; d += THREADS) {
-      uint32_t run = 0;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        const uint32_t c = s_hist[w * RADIX + d];
-        s_hist[w * RADIX + d] = run;
-        run += c;
+      uint32_t excl = 0;
+      int k = row - 1;
+      uint32_t spin = 0;
+      while (true) {
+        uint32_t v[kLookback];
+  #pragma unroll
+        for (int q = 0; q < kLookback; ++q)
+          v[q] = ld_relaxed(desc + size_t(max(k - q, init_row)) * RADIX + d);
+        int used = 0;
+        bool done = false;
+  #pragma unroll
+        for (int q = 0; q < kLookback; ++q) {
+          const uint32_t f = v[q] & kFlagMask;
+          if (done || f == 0 || used != q) break;
+          excl += v[q] >> 2;
+          ++used;
+          done = f == kFlagInc;
+        }
+        if (done) break;
+        if (used) {
+          k -= used;
+          spin = 0;
+          continue;
+        }
+        if (++spin > spin_limit || device_failed(st)) {
+          report_error(st, RW_ERR_TIMEOUT, kSiteSort);
+          break;
+        }
+        backoff(spin);
       }
-      s_cnt[d] = run;
-      st_relaxed(drow + d, kFlagAgg | (run << 2));
+      st_relaxed(drow + d, kFlagInc | ((excl + s_cnt[d]) << 2));
+      s_gofs[d] = excl - s_start[d];
     }
-  }
-  __syncthreads();
-  digit_exclusive_scan<D, THREADS>(s_cnt, s_start, s_misc + 1);
-  __syncthreads();
-  // fold the digit starts into the per-warp offsets once per tile, so that
-  // placing a key below reads one shared-memory word instead of two
-  if (RANK == kRankHalfPacked) {
-    for (int i = tid; i < 2 * NW * RADIX; i += THREADS)
-      s_hist[i] += s_start[(i >> 1) & (RADIX - 1)];
-  } else {
-    for (int i = tid; i < NW * RADIX; i += THREADS) s_hist[i] += s_start[i & (RADIX - 1)];
-  }
-  __syncthreads();
+    __syncthreads();
 
-  // reorder the tile by digit in shared memory first: it needs only the
-  // tile's own counts, and gives the predecessors time to publish their
-  // inclusive prefixes before the look-back below reads them
-  if (RANK == kRankHalfPacked) {
-    if (full) half_place<D, KPT, true>(keys, rank2, shift, hbase, n, wp, s_keys);
-    else half_place<D, KPT, false>(keys, rank2, shift, hbase, n, wp, s_keys);
-  } else if (full) {
-    warp_place<D, KPT, true>(keys, rank2, shift, wbase, n, wh, s_keys);
-  } else {
-    warp_place<D, KPT, false>(keys, rank2, shift, wbase, n, wh, s_keys);
-  }
-
-  // decoupled look-back, kLookback descriptors per round trip.  The segment's
-  // first row is always inclusive, so rows are read clamped to it and the
-  // walk stops there at the latest.
-  for (int d = tid; d < RADIX; d += THREADS) {
-    uint32_t excl = 0;
-    int k = row - 1;
-    uint32_t spin = 0;
-    while (true) {
-      uint32_t v[kLookback];
-#pragma unroll
-      for (int q = 0; q < kLookback; ++q)
-        v[q] = ld_relaxed(desc + size_t(max(k - q, init_row)) * RADIX + d);
-      int used = 0;
-      bool done = false;
-#pragma unroll
-      for (int q = 0; q < kLookback; ++q) {
-        const uint32_t f = v[q] & kFlagMask;
-        if (done || f == 0 || used != q) break;
-        excl += v[q] >> 2;
-        ++used;
-        done = f == kFlagInc;
+    // write runs of equal digits to their global positions (a destination is
+    // out of range only if a look-back gave up)
+    const uint32_t total = seg.total;
+    if (full) {
+  #pragma unroll 4
+      for (int i = 0; i < KPT; ++i) {
+        const uint32_t p = tid + uint32_t(i) * THREADS;
+        const K k = s_keys[p];
+        const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
+        if (dst < total) out[dst] = k;
       }
-      if (done) break;
-      if (used) {
-        k -= used;
-        spin = 0;
-        continue;
+    } else {
+      const uint32_t tile_n = n - base;
+      for (uint32_t p = tid; p < tile_n; p += THREADS) {
+        const K k = s_keys[p];
+        const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
+        if (dst < total) out[dst] = k;
       }
-      if (++spin > spin_limit || device_failed(st)) {
-        report_error(st, RW_ERR_TIMEOUT, kSiteSort);
-        break;
-      }
-      backoff(spin);
     }
-    st_relaxed(drow + d, kFlagInc | ((excl + s_cnt[d]) << 2));
-    s_gofs[d] = excl - s_start[d];
-  }
-  __syncthreads();
-
-  // write runs of equal digits to their global positions (a destination is
-  // out of range only if a look-back gave up)
-  const uint32_t total = seg.total;
-  if (full) {
-#pragma unroll 4
-    for (int i = 0; i < KPT; ++i) {
-      const uint32_t p = tid + uint32_t(i) * THREADS;
-      const K k = s_keys[p];
-      const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
-      if (dst < total) out[dst] = k;
-    }
-  } else {
-    const uint32_t tile_n = n - base;
-    for (uint32_t p = tid; p < tile_n; p += THREADS) {
-      const K k = s_keys[p];
-      const uint32_t dst = s_gofs[uint32_t(k >> shift) & (RADIX - 1)] + p;
-      if (dst < total) out[dst] = k;
-    }
+    if (!PERSIST) break;
+    __syncthreads();  // the next tile reuses every shared array
   }
 }
 
@@ -416,7 +426,10 @@ template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
                      cudaEvent_t* marks, uint32_t probe_spins) {
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
-  auto kern = k_binning<K, D, THREADS, KPT, RANK, MINB>;
+  // a gated sort (a fallback that may not be needed) runs persistent passes
+  const bool persist = sc.gate != nullptr && !probe_spins;
+  auto kern = persist ? k_binning<K, D, THREADS, KPT, RANK, MINB, true>
+                      : k_binning<K, D, THREADS, KPT, RANK, MINB, false>;
   const uint32_t tiles = pl.sort_map.n_tiles;
   if (tiles + pl.seg.count > sc.sort_rows) return cudaErrorInvalidValue;
   launch_pdl(k_sort_init<D>, pl.seg.count * sc.passes, 256, 0, s, sc.ghist, sc.sort_desc, pl.seg,
@@ -442,10 +455,12 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
     return cudaGetLastError();
   }
   const K* src = keys;
+  const uint32_t grid =
+      persist ? std::min<uint32_t>(tiles, uint32_t(sc.num_sms) * uint32_t(MINB)) : tiles;
   for (int p = 0; p < sc.passes; ++p) {
     K* dst = ((sc.passes - 1 - p) % 2 == 0) ? alt : tmp;
     if (tiles)
-      launch_pdl(kern, tiles, THREADS, C::kSmem, s, 
+      launch_pdl(kern, grid, THREADS, C::kSmem, s, 
           src, dst, pl.seg, pl.sort_map, p * D,
           sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
           sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit, sc.gate);
