@@ -412,17 +412,17 @@ struct GlobalKeys {
 //
 // L and R per gap: in chunks of 32 gaps (one per lane) a bit-serial warp
 // comparison of E = D + 1 (0 marks the walls at -1 and n) gives every lane
-// the lanes with a smaller value, hence the nearest smaller in the chunk; the
-// ballots of the comparison (the chunk's bit planes of E) are kept.  Across
-// the tile and a halo of kAnsvHalo chunks on either side, per-value bitmasks
-// of the chunks whose minimum lies below v find the nearest such chunk in one
-// clz / ffs, and the same bit-serial comparison over that chunk's planes
-// gives its last / first lane below v; a gap whose nearest smaller lies
-// beyond the halo (a node near the top of the tree) goes to a list that a
+// the lanes with a smaller value, hence the nearest smaller in the chunk, and
+// every value v the last / first position in the chunk below v.  Across the
+// tile and a halo of kAnsvHalo chunks on either side, per-value bitmasks of
+// the chunks whose minimum lies below v find the nearest such chunk in one
+// clz / ffs, and its summary gives the answer; a gap whose nearest smaller
+// lies beyond the halo (a node near the top of the tree) goes to a list that a
 // second kernel resolves with warp-cooperative searches of the keys.
 constexpr int kAnsvHalo = 8;                                        // chunks per side
 constexpr int kAnsvChunks = int(kTreeTile) / 32 + 2 * kAnsvHalo;   // chunks per window
 constexpr int kAnsvWin = kAnsvChunks * 32;                           // gaps per window
+constexpr int kAnsvRow = kAnsvChunks + 1;  // padded: lane v and chunk c in different banks
 constexpr int kAnsvNone = -0x7fffffff;     // "no smaller gap found to the left"
 constexpr int kAnsvNoneR = 0x7fffffff;     // "none to the right"
 
@@ -432,30 +432,9 @@ struct AnsvCfg {
   static constexpr int VB = sizeof(K) == 4 ? 5 : 6;    // bits of E
   static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
   static constexpr int MW = (kAnsvChunks + 31) / 32;  // mask words per value
-  static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 +
-                                  size_t(kAnsvChunks) * VB * 4 + 2 * size_t(kTreeTile) +
-                                  size_t(kAnsvWin) + size_t(kAnsvChunks);
+  static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 + 2 * size_t(NV) * kAnsvRow +
+                                  2 * size_t(kTreeTile) + size_t(kAnsvWin) + size_t(kAnsvChunks);
 };
-
-// Lanes of a chunk whose E is below v, from the chunk's bit planes (plane b:
-// the ballot of bit b of E over the chunk's 32 lanes), bit-serially from the
-// top bit: a lane is below v at the first bit where the two differ and v has
-// the 1.
-template <int VB>
-__device__ __forceinline__ uint32_t lanes_below(const uint32_t* planes, int v) {
-  uint32_t lt = 0, eq = 0xffffffffu;
-#pragma unroll
-  for (int bt = VB - 1; bt >= 0; --bt) {
-    const uint32_t P = planes[bt];
-    if ((v >> bt) & 1) {
-      lt |= eq & ~P;
-      eq &= P;
-    } else {
-      eq &= ~P;
-    }
-  }
-  return lt;
-}
 
 // Warp-cooperative search for the nearest smaller gaps of gap g beyond any
 // window, both sides in lockstep: 32 probes per side and round (doubling
@@ -552,8 +531,9 @@ __global__ void __launch_bounds__(kTreeThreads)
   // positions inside a chunk are kept as lane indices (0xff: none)
   K* s_key = reinterpret_cast<K*>(smem_raw);                                   // [kAnsvWin + 1]
   uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw + C::kKeyBytes);     // [NV][MW]
-  uint32_t* s_plane = s_mask + NV * C::MW;                                     // [chunks][VB]
-  uint8_t* s_lp = reinterpret_cast<uint8_t*>(s_plane + kAnsvChunks * VB);      // [kTreeTile]
+  uint8_t* s_last = reinterpret_cast<uint8_t*>(s_mask + NV * C::MW);           // [NV][kAnsvRow]
+  uint8_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
+  uint8_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
   uint8_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
   uint8_t* s_e = s_rp + kTreeTile;                                             // [kAnsvWin]
   uint8_t* s_cmin = s_e + kAnsvWin;                                            // [kAnsvChunks]
@@ -595,9 +575,8 @@ __global__ void __launch_bounds__(kTreeThreads)
   }
   __syncthreads();
 
-  // phase A: per chunk, E, the nearest smaller inside the chunk on either
-  // side, and the chunk's bit planes (what the lookups of other chunks' gaps
-  // need: lanes_below over them gives the chunk's lanes below any value)
+  // phase A: per chunk, E, the nearest smaller inside the chunk, and the
+  // chunk's summaries (last / first position with E below each value)
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   static_assert(C::kKeyBytes % 4 == 0, "the masks follow the keys");
   // two chunks at a time per warp, so that their ballot chains interleave
@@ -615,32 +594,44 @@ __global__ void __launch_bounds__(kTreeThreads)
       const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e[j]));
       if (lane == 0) s_cmin[ch] = uint8_t(cmin);
     }
-    // bit-serial comparison of every lane's E against its own value, with the
-    // ballots of each bit: lt ends as the lanes of the chunk below my E
-    uint32_t lt[2] = {0, 0}, eq[2] = {0xffffffffu, 0xffffffffu};
+    // bit-serial comparison of every lane's E against v = lane (and lane + 32
+    // for 64-bit keys): lane v ends with the lanes whose E is below v; the
+    // lanes below my own value are then lane e's result
+    uint32_t lt0[2] = {0, 0}, eq0[2] = {0xffffffffu, 0xffffffffu};  // below v = lane
+    uint32_t lt1[2] = {0, 0}, eq1[2] = {0xffffffffu, 0xffffffffu};  // below v = lane + 32
 #pragma unroll
     for (int bt = VB - 1; bt >= 0; --bt) {
+      uint32_t B[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) B[j] = __ballot_sync(0xffffffffu, (e[j] >> bt) & 1);
+      const bool b0 = (int(lane) >> bt) & 1, b1 = ((int(lane) + 32) >> bt) & 1;
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const bool mine = (e[j] >> bt) & 1;
-        const uint32_t B = __ballot_sync(0xffffffffu, mine);
-        if (lane == uint32_t(bt)) s_plane[(ch0 + j * NW) * VB + bt] = B;
-        if (mine) {
-          lt[j] |= eq[j] & ~B;
-          eq[j] &= B;
-        } else {
-          eq[j] &= ~B;
+        if (b0) { lt0[j] |= eq0[j] & ~B[j]; eq0[j] &= B[j]; } else { eq0[j] &= ~B[j]; }
+        if (NV > 32) {
+          if (b1) { lt1[j] |= eq1[j] & ~B[j]; eq1[j] &= B[j]; } else { eq1[j] &= ~B[j]; }
         }
       }
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int ch = ch0 + j * NW;
+      const uint32_t from0 = __shfl_sync(0xffffffffu, lt0[j], e[j] & 31);
+      const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1[j], e[j] & 31) : 0u;
+      const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
       if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
         const int tg = (ch - kAnsvHalo) * 32 + int(lane);
-        const uint32_t lm = lt[j] & lanemask_lt(), rm = lt[j] & ~lanemask_lt() & ~(1u << lane);
+        const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
         s_lp[tg] = lm ? uint8_t(31 - __clz(lm)) : uint8_t(0xff);
         s_rp[tg] = rm ? uint8_t(__ffs(rm) - 1) : uint8_t(0xff);
+      }
+      s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(31 - __clz(lt0[j])) : uint8_t(0xff);
+      s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(__ffs(lt0[j]) - 1) : uint8_t(0xff);
+      if (NV > 32) {
+        s_last[(int(lane) + 32) * kAnsvRow + ch] =
+            lt1[j] ? uint8_t(31 - __clz(lt1[j])) : uint8_t(0xff);
+        s_first[(int(lane) + 32) * kAnsvRow + ch] =
+            lt1[j] ? uint8_t(__ffs(lt1[j]) - 1) : uint8_t(0xff);
       }
     }
   }
@@ -660,8 +651,10 @@ __global__ void __launch_bounds__(kTreeThreads)
 
   // phase C: every gap of the tile writes its node; a gap whose nearest
   // smaller gap lies beyond the window goes to the far-search list
-  // D of a gap of [0, n): every L and R found here lies inside the window
-  auto d_at = [&](int p) -> int { return int(s_e[p - wlo]) - 1; };
+  const int wend = wlo + kAnsvWin - 1;  // last gap of the window
+  auto d_at = [&](int p) -> int {       // D of gap p in [0, n)
+    return (p >= wlo && p <= wend) ? int(s_e[p - wlo]) - 1 : delta(codes[p], codes[p + 1]);
+  };
   for (int tg = int(threadIdx.x); tg < int(kTreeTile); tg += kTreeThreads) {
     const int g = g0 + tg;
     if (g >= n) break;
@@ -677,7 +670,7 @@ __global__ void __launch_bounds__(kTreeThreads)
         if (wd == (ch - 1) >> 5) bits &= 0xffffffffu >> (31 - ((ch - 1) & 31));
         if (bits) {
           const int c2 = wd * 32 + 31 - __clz(bits);
-          L = wlo + c2 * 32 + 31 - __clz(lanes_below<VB>(s_plane + c2 * VB, e));
+          L = wlo + c2 * 32 + s_last[e * kAnsvRow + c2];
           break;
         }
       }
@@ -689,7 +682,7 @@ __global__ void __launch_bounds__(kTreeThreads)
         if (wd == (ch + 1) >> 5) bits &= 0xffffffffu << ((ch + 1) & 31);
         if (bits) {
           const int c2 = wd * 32 + __ffs(bits) - 1;
-          R = wlo + c2 * 32 + __ffs(lanes_below<VB>(s_plane + c2 * VB, e)) - 1;
+          R = wlo + c2 * 32 + s_first[e * kAnsvRow + c2];
           break;
         }
       }
