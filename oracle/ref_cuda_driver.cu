@@ -40,6 +40,12 @@
 #include <string>
 
 #include "app_data.hpp"
+#include "cuda/01_morton.cuh"
+#include "cuda/03_unique.cuh"
+#include "cuda/04_radix_tree.cuh"
+#include "cuda/05_edge_count.cuh"
+#include "cuda/06_prefix_sum.cuh"
+#include "cuda/07_octree.cuh"
 #include "cuda/cu_dispatcher.cuh"
 #include "cuda/im_storage.cuh"
 #include "redwood/cuda/cu_mem_resource.cuh"
@@ -109,6 +115,41 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 
 extern "C" {
+
+// Launch-free look at the reference's kernels that its headers declare:
+// cudaFuncGetAttributes on each, one line per kernel into out (for a kernel
+// the runtime cannot find, the error text).  Returns 0.
+int refcu_kernel_report(char* out, int out_len) {
+  std::string r;
+  auto one = [&](const char* name, const void* fn) {
+    cudaFuncAttributes a{};
+    const cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    r += std::string(name) + ": ";
+    if (e != cudaSuccess) {
+      r += cudaGetErrorString(e);
+      cudaGetLastError();
+    } else {
+      r += "regs " + std::to_string(a.numRegs) + ", static smem " +
+           std::to_string(a.sharedSizeBytes) + ", max threads " +
+           std::to_string(a.maxThreadsPerBlock) + ", ptx " + std::to_string(a.ptxVersion) +
+           ", binary " + std::to_string(a.binaryVersion);
+    }
+    r += "\n";
+  };
+  one("k_ComputeMortonCode", reinterpret_cast<const void*>(cuda::kernels::k_ComputeMortonCode));
+  one("k_FindDups", reinterpret_cast<const void*>(cuda::kernels::k_FindDups));
+  one("k_BuildRadixTree", reinterpret_cast<const void*>(cuda::kernels::k_BuildRadixTree));
+  one("k_EdgeCount", reinterpret_cast<const void*>(cuda::kernels::k_EdgeCount));
+  one("k_SingleBlockExclusiveScan<int>",
+      reinterpret_cast<const void*>(cuda::kernels::k_SingleBlockExclusiveScan<int>));
+  one("k_PrefixSumLocal<int>", reinterpret_cast<const void*>(cuda::kernels::k_PrefixSumLocal<int>));
+  one("k_MakeOctNodes", reinterpret_cast<const void*>(cuda::kernels::k_MakeOctNodes));
+  if (out && out_len > 0) {
+    std::strncpy(out, r.c_str(), size_t(out_len) - 1);
+    out[out_len - 1] = '\0';
+  }
+  return 0;
+}
 
 // Times `iters` runs of the reference's cuda::run_stage1..7 on the cloud
 // pts[4 n] (copied into the AppData's managed input once).  per_iter_ms gets

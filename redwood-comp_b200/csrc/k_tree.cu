@@ -589,7 +589,8 @@ __global__ void __launch_bounds__(kTreeThreads)
       const int w = ch * 32 + int(lane);  // window index of this lane's gap
       const int g = wlo + w;
       const bool real = g >= 0 && g < n;
-      e[j] = real ? max(delta(s_key[w], s_key[w + 1]) + 1, 0) : 0;
+      // distinct keys: delta >= 0, so a real gap's E >= 1 and 0 marks walls only
+      e[j] = real ? delta(s_key[w], s_key[w + 1]) + 1 : 0;
       s_e[w] = uint8_t(e[j]);
       const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e[j]));
       if (lane == 0) s_cmin[ch] = uint8_t(cmin);
@@ -597,6 +598,9 @@ __global__ void __launch_bounds__(kTreeThreads)
     // bit-serial comparison of every lane's E against v = lane (and lane + 32
     // for 64-bit keys): lane v ends with the lanes whose E is below v; the
     // lanes below my own value are then lane e's result
+    // (branch-free: with m = all ones where v has the bit, a lane stays equal
+    // while its bit matches, eq &= ~(B ^ m), and falls below where v has the
+    // bit and it has not, lt |= eq & ~B & m)
     uint32_t lt0[2] = {0, 0}, eq0[2] = {0xffffffffu, 0xffffffffu};  // below v = lane
     uint32_t lt1[2] = {0, 0}, eq1[2] = {0xffffffffu, 0xffffffffu};  // below v = lane + 32
 #pragma unroll
@@ -604,12 +608,14 @@ __global__ void __launch_bounds__(kTreeThreads)
       uint32_t B[2];
 #pragma unroll
       for (int j = 0; j < 2; ++j) B[j] = __ballot_sync(0xffffffffu, (e[j] >> bt) & 1);
-      const bool b0 = (int(lane) >> bt) & 1, b1 = ((int(lane) + 32) >> bt) & 1;
+      const uint32_t m0 = 0u - ((lane >> bt) & 1u), m1 = 0u - (((lane + 32u) >> bt) & 1u);
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        if (b0) { lt0[j] |= eq0[j] & ~B[j]; eq0[j] &= B[j]; } else { eq0[j] &= ~B[j]; }
+        lt0[j] |= eq0[j] & ~B[j] & m0;
+        eq0[j] &= ~(B[j] ^ m0);
         if (NV > 32) {
-          if (b1) { lt1[j] |= eq1[j] & ~B[j]; eq1[j] &= B[j]; } else { eq1[j] &= ~B[j]; }
+          lt1[j] |= eq1[j] & ~B[j] & m1;
+          eq1[j] &= ~(B[j] ^ m1);
         }
       }
     }
