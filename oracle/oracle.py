@@ -338,7 +338,7 @@ class RefTreeCuda:
         points = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
         n = points.shape[0]
         ms = np.zeros(iters, np.float64)
-        info = np.zeros(6, np.uint32)
+        info = np.zeros(7, np.uint32)
         err = ctypes.create_string_buffer(512)
         rc = self.lib.refcu_time(_ptr(points), ctypes.c_uint32(n), ctypes.c_int(iters),
                                  _ptr(ms), _ptr(info), err, ctypes.c_int(512))
@@ -348,7 +348,8 @@ class RefTreeCuda:
                 "rows_out_of_range": int(info[1]), "parents_out_of_range": int(info[2]),
                 "n_unique": int(info[3]),
                 "n_octree_nodes": None if info[4] == 0xFFFFFFFF else int(info[4]),
-                "stage4_input_unsorted": bool(info[5])}
+                "stage4_input_unsorted": bool(info[5]),
+                "stage6_launched_by_driver": bool(info[6])}
 
 
 def compare(a: TreeResult, b: TreeResult) -> list[str]:

@@ -96,6 +96,49 @@ __device__ __forceinline__ void backoff(uint32_t spin) {
   if (spin > 64) __nanosleep(spin > 4096 ? 512 : 64);
 }
 
+// ---- bulk copies global -> shared (cp.async.bulk) completed on an mbarrier ----
+// One thread arms the barrier with the byte count and issues the copy; every
+// thread then waits for the barrier's phase 0.  Source, destination and size
+// must be multiples of 16 bytes (the caller checks).
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Initialises the barrier (one arrival per phase) and makes the initialisation
+// visible to the copy engine; call from one thread, then __syncthreads().
+__device__ __forceinline__ void bulk_barrier_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One thread: expect `bytes` on the barrier and copy them from global memory.
+__device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst_smem)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// Waits for phase 0 of the barrier, at most `limit` polls (with back-off);
+// returns false if the copy did not complete in time.
+__device__ __forceinline__ bool bulk_wait(uint64_t* bar, uint32_t limit) {
+  const uint32_t a = smem_addr(bar);
+  for (uint32_t spin = 0; spin < limit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done) : "r"(a) : "memory");
+    if (done) return true;
+    backoff(spin);
+  }
+  return false;
+}
+
 // Inclusive warp scan (Kogge-Stone over shuffles).
 template <typename T>
 __device__ __forceinline__ T warp_inclusive_scan(T v) {

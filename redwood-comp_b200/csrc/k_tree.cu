@@ -517,7 +517,7 @@ __device__ __forceinline__ void write_gap_node(int g, int n, int D, int L, int R
 }
 
 template <typename K, bool EDGES>
-__global__ void __launch_bounds__(kTreeThreads)
+__global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per SM
     k_radix_tree(const K* __restrict__ codes_all, SegTable seg, TileMap map,
                  const uint32_t* __restrict__ n_unique, int32_t* __restrict__ seg_err,
                  uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
@@ -569,9 +569,32 @@ __global__ void __launch_bounds__(kTreeThreads)
     if (EDGES) edge_count[sb] = 0;
   }
 
-  for (int j = threadIdx.x; j <= kAnsvWin; j += kTreeThreads) {
-    const int k = wlo + j;
-    s_key[j] = (k >= 0 && k <= n) ? codes[k] : K(0);
+  // the window's keys [wlo, wlo + kAnsvWin]: one bulk copy when the window
+  // lies inside the keys and starts on a 16-byte boundary (every interior
+  // tile of a plain run), else key by key with zeros outside [0, n]
+  static_assert((size_t(kAnsvWin) * sizeof(K)) % 16 == 0, "bulk copies move 16-byte units");
+  __shared__ __align__(8) uint64_t s_bar;
+  const bool bulk = wlo >= 0 && wlo + kAnsvWin <= n &&
+                    (reinterpret_cast<uintptr_t>(codes + wlo) & 15u) == 0;
+  if (bulk) {
+    if (threadIdx.x == 0) bulk_barrier_init(&s_bar);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      bulk_load(s_key, codes + wlo, uint32_t(kAnsvWin * sizeof(K)), &s_bar);
+      s_key[kAnsvWin] = codes[wlo + kAnsvWin];
+    }
+    const bool landed = bulk_wait(&s_bar, kSpinLimit);
+    if (__syncthreads_or(!landed)) {  // the whole block gives up together
+      // report, and let the copy land before the block's shared memory goes
+      if (threadIdx.x == 0) seg_error(seg_err, c, RW_ERR_TIMEOUT);
+      bulk_wait(&s_bar, kSpinLimit);
+      return;
+    }
+  } else {
+    for (int j = threadIdx.x; j <= kAnsvWin; j += kTreeThreads) {
+      const int k = wlo + j;
+      s_key[j] = (k >= 0 && k <= n) ? codes[k] : K(0);
+    }
   }
   __syncthreads();
 
