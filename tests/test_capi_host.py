@@ -66,3 +66,18 @@ def test_generators(rw):
     # multithreaded generation is chunk-independent
     big = rw.generate_points(300000, rw.GEN_GAUSSIAN_MIXTURE, 9, n_components=32)
     assert np.array_equal(big[:200000], g)
+
+
+def test_new_entry_points_validate_before_the_device(rw):
+    """The entry points added for options, the bounded-wait probe and the
+    batch's learned stage 2 reject bad arguments before any device access."""
+    lib = rw.lib()
+    assert lib.rw_tree_im_storage_set_options(None, 0) == rw.RW_ERR_ARG
+    assert lib.rw_tree_sort_lookback_probe(None, None, 64, None) == rw.RW_ERR_ARG
+    assert lib.rw_tree_batch_set_learned(None, None, 0, None) == rw.RW_ERR_ARG
+    assert lib.rw_tree_learned_sort(None, None, None, 0, 0, None, None, None) == rw.RW_ERR_ARG
+    # the option bits and the learned modes the header defines
+    text = open(os.path.join(ROOT, "include", "rw_tree.h")).read()
+    assert "#define RW_TREE_OPT_GEOMETRIC_DELTA 1" in text
+    assert "#define RW_TREE_OPT_LINK_LEAVES 2" in text
+    assert (rw.OPT_GEOMETRIC_DELTA, rw.OPT_LINK_LEAVES) == (1, 2)
