@@ -339,9 +339,10 @@ class RefTreeCuda:
         n = points.shape[0]
         ms = np.zeros(iters, np.float64)
         info = np.zeros(7, np.uint32)
+        stage_ms = np.zeros(7, np.float64)
         err = ctypes.create_string_buffer(512)
         rc = self.lib.refcu_time(_ptr(points), ctypes.c_uint32(n), ctypes.c_int(iters),
-                                 _ptr(ms), _ptr(info), err, ctypes.c_int(512))
+                                 _ptr(ms), _ptr(info), _ptr(stage_ms), err, ctypes.c_int(512))
         if rc:
             raise RuntimeError(f"refcu_time: status {rc} {err.value.decode()}")
         return {"ms": ms.tolist(), "all_stages_ran": bool(info[0]),
@@ -349,7 +350,8 @@ class RefTreeCuda:
                 "n_unique": int(info[3]),
                 "n_octree_nodes": None if info[4] == 0xFFFFFFFF else int(info[4]),
                 "stage4_input_unsorted": bool(info[5]),
-                "stage6_launched_by_driver": bool(info[6])}
+                "stage6_did_not_launch": bool(info[6]),
+                "stage_ms_last_run": [round(float(x), 4) for x in stage_ms]}
 
 
 def compare(a: TreeResult, b: TreeResult) -> list[str]:

@@ -110,19 +110,6 @@ void stage_done(int k) {
                              cudaGetErrorString(e));
 }
 
-// The body of the reference's run_stage6 (cu_dispatcher.cu:672-686): its
-// single-block exclusive scan kernel with the same configuration and
-// arguments, then n_octree_nodes = edge_offset[n_brt - 1] as it sets it.
-void run_stage6_here(AppData& app, cudaStream_t stream) {
-  constexpr auto n_threads = cuda::agents::PrefixSumAgent<int>::n_threads;
-  cuda::kernels::k_SingleBlockExclusiveScan<<<1, n_threads, 0, stream>>>(
-      app.u_edge_count.data(), app.u_edge_offset.data(),
-      static_cast<int>(app.get_n_brt_nodes()));
-  stage_done(6);
-  CUDA_CHECK(cudaStreamSynchronize(stream));
-  app.set_n_octree_nodes(app.u_edge_offset[app.get_n_brt_nodes() - 1]);
-}
-
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
       .count();
@@ -169,16 +156,19 @@ int refcu_kernel_report(char* out, int out_len) {
 
 // Times `iters` runs of the reference's cuda::run_stage1..7 on the cloud
 // pts[4 n] (copied into the AppData's managed input once).  per_iter_ms gets
-// each run's wall time (the stages that ran, checks excluded).  info[0] = 1
+// each run's wall time (the stages that ran, checks excluded), stage_ms[7]
+// the last run's time of each stage (0 for one that did not run).  info[0] = 1
 // when every stage ran in every run, info[1] = octree rows out of range found
 // by the stage-7 check (last run), info[2] = parent indices out of range,
 // info[3] = the reference's n_unique, info[4] = its n_octree_nodes (last
 // run), info[5] = 1 when stage 4's input was not strictly increasing,
-// info[6] = 1 when stage 6's kernel had to be launched by this driver.
+// info[6] = 1 when stage 6's kernel did not launch (stages 6 and 7 then
+// did not run).
 // Returns 0, 1 for bad arguments, 2 for a CUDA error (text in err).
 int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uint32_t* info,
-               char* err, int err_len) {
-  if (!pts || n < 1024 || n % 1024 != 0 || iters < 1 || !per_iter_ms || !info) return 1;
+               double* stage_ms, char* err, int err_len) {
+  if (!pts || n < 1024 || n % 1024 != 0 || iters < 1 || !per_iter_ms || !info || !stage_ms)
+    return 1;
   try {
     cudaStream_t stream;
     CUDA_CHECK(cudaStreamCreate(&stream));
@@ -194,7 +184,6 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
       unsigned host_flags[2] = {0, 0};
       info[5] = 0;
       info[6] = 0;
-      bool stage6_from_driver = false;
       uint32_t last_m = 0xffffffffu;
       auto check = [&](auto launch) {
         CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned), stream));
@@ -205,18 +194,29 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
         CUDA_CHECK(cudaStreamSynchronize(stream));
         return host_flags[0] == 0 && host_flags[1] == 0;
       };
+      for (int s = 0; s < 7; ++s) stage_ms[s] = 0.0;
+      // one reference stage, its wall time (it synchronises itself) into
+      // stage_ms[k - 1] (the last run's) and into this run's total
+      double ms = 0.0;
+      auto stage = [&](int k, auto fn) {
+        const auto t0 = std::chrono::steady_clock::now();
+        fn();
+        stage_done(k);
+        const double x = ms_since(t0);
+        stage_ms[k - 1] = x;
+        ms += x;
+      };
       for (int it = 0; it < iters; ++it) {
-        auto t0 = std::chrono::steady_clock::now();
-        cuda::run_stage1(app, stream);
-        stage_done(1);
-        cuda::run_stage2(app, im, stream);
-        stage_done(2);
-        CUDA_CHECK(cudaMemcpyAsync(app.u_morton_keys_alt.data(), app.u_morton_keys.data(),
-                                   size_t(4) * n, cudaMemcpyDeviceToDevice, stream));
-        CUDA_CHECK(cudaStreamSynchronize(stream));
-        cuda::run_stage3(app, im, stream);
-        stage_done(3);
-        double ms = ms_since(t0);
+        ms = 0.0;
+        stage(1, [&] { cuda::run_stage1(app, stream); });
+        stage(2, [&] {
+          cuda::run_stage2(app, im, stream);
+          stage_done(2);
+          CUDA_CHECK(cudaMemcpyAsync(app.u_morton_keys_alt.data(), app.u_morton_keys.data(),
+                                     size_t(4) * n, cudaMemcpyDeviceToDevice, stream));
+          CUDA_CHECK(cudaStreamSynchronize(stream));
+        });
+        stage(3, [&] { cuda::run_stage3(app, im, stream); });
         const int nu = static_cast<int>(app.get_n_unique());
         const bool sorted = nu >= 3 && nu <= static_cast<int>(n) && check([&] {
           k_check_increasing<<<148 * 4, 256, 0, stream>>>(app.u_morton_keys.data(), nu, flags);
@@ -227,40 +227,34 @@ int refcu_time(const float* pts, uint32_t n, int iters, double* per_iter_ms, uin
           per_iter_ms[it] = ms;
           continue;
         }
-        t0 = std::chrono::steady_clock::now();
-        cuda::run_stage4(app, stream);
-        stage_done(4);
-        cuda::run_stage5(app, stream);
-        stage_done(5);
-        if (!stage6_from_driver) {
+        stage(4, [&] { cuda::run_stage4(app, stream); });
+        stage(5, [&] { cuda::run_stage5(app, stream); });
+        {
+          const auto t0 = std::chrono::steady_clock::now();
           cuda::run_stage6(app, stream);
           const cudaError_t e6 = cudaGetLastError();
           if (e6 == cudaErrorInvalidDeviceFunction) {
-            // its dispatcher's launch of the scan template finds no device
-            // function on this build, the same kernel launched here does
-            stage6_from_driver = true;
+            // its single-block scan kernel does not launch on this device
+            // (the runtime finds the function, its launch reports this); the
+            // count it would set is not trusted and stage 7 is not run
+            all_ran = false;
             info[6] = 1;
-          } else if (e6 != cudaSuccess) {
-            throw std::runtime_error(std::string("reference stage 6: ") +
-                                     cudaGetErrorString(e6));
+            per_iter_ms[it] = ms;
+            continue;
           }
+          if (e6 != cudaSuccess)
+            throw std::runtime_error(std::string("reference stage 6: ") + cudaGetErrorString(e6));
+          stage_ms[5] = ms_since(t0);
+          ms += stage_ms[5];
         }
-        if (stage6_from_driver) run_stage6_here(app, stream);
-        ms += ms_since(t0);
         last_m = app.get_n_octree_nodes();
         const bool rows_ok = check([&] {
           k_check_stage7<<<148 * 4, 256, 0, stream>>>(
               app.u_edge_offset.data(), app.u_edge_count.data(), app.brt.u_parents.data(),
               static_cast<int>(app.get_n_brt_nodes()), static_cast<int>(n), rows, flags);
         });
-        if (rows_ok) {
-          t0 = std::chrono::steady_clock::now();
-          cuda::run_stage7(app, stream);
-          stage_done(7);
-          ms += ms_since(t0);
-        } else {
-          all_ran = false;
-        }
+        if (rows_ok) stage(7, [&] { cuda::run_stage7(app, stream); });
+        else all_ran = false;
         per_iter_ms[it] = ms;
       }
       info[0] = all_ran ? 1u : 0u;
