@@ -613,6 +613,26 @@ def ref_cuda_isolated(a, warmup=2, iters=10):
     return out
 
 
+def rank_barrier(world):
+    """Every rank waits for the others (the timed regions start and end
+    together); nothing with one process."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def rank_max(x, world, device):
+    """The largest of every rank's x (each rank's step time: the job's time is
+    its slowest rank's), the same value on every rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def port_time(pts, a, iters):
     from oracle import Oracle
     orc = Oracle()
@@ -680,15 +700,10 @@ def main():
     passes = sort_passes(a)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, world, "cuda")
 
     stream = torch.cuda.current_stream()
     for _ in range(a.warmup):

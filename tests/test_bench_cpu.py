@@ -86,3 +86,35 @@ def test_reference_arm_loads_no_product_library():
     assert ref_line["config"] == probe["config"]
     assert set(probe["config"]) >= {"workload", "n_points", "key_bits", "radix_bits",
                                     "sort_passes", "parallelism"}
+
+
+def _two_rank_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    bench = load_bench()
+    bench.rank_barrier(world)
+    step_ms = [1.5, 4.25][rank]  # each rank's own step time
+    out[rank] = bench.rank_max(step_ms, world, "cpu")
+    bench.rank_barrier(world)
+    dist.destroy_process_group()
+
+
+def test_two_ranks_take_the_slowest_step():
+    """The replicas-only multi-GPU path: with world size 2 (gloo, CPU) both
+    ranks pass the barriers and agree on the slowest rank's step time, which
+    bench.py divides the whole job's points by."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_two_rank_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0] == out[1] == 4.25
