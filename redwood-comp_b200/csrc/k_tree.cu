@@ -569,6 +569,10 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
     if (EDGES) edge_count[sb] = 0;
   }
 
+  __shared__ uint32_t s_far[kTreeFarPerTile];  // the tile's gaps left to phase D
+  __shared__ uint32_t s_far_n;
+  if (threadIdx.x == 0) s_far_n = 0;  // read after the barriers below
+
   // the window's keys [wlo, wlo + kAnsvWin]: one bulk copy when the window
   // lies inside the keys and starts on a 16-byte boundary (every interior
   // tile of a plain run), else key by key with zeros outside [0, n]
@@ -717,6 +721,13 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       }
     }
     if (L == kAnsvNone || R == kAnsvNoneR) {
+      // resolved by this block below (at most kTreeFarPerTile per tile); the
+      // global list and k_radix_tree_far only if that ever overflowed
+      const uint32_t local = atomicAdd(&s_far_n, 1u);
+      if (local < kTreeFarPerTile) {
+        s_far[local] = uint32_t(g);
+        continue;
+      }
       const uint32_t slot = atomicAdd(far_n, 1u);
       if (slot < far_cap) {
         far[2 * slot] = sb + uint32_t(g);
@@ -727,6 +738,23 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
     write_gap_node<K, EDGES>(g, n, e - 1, max(L, -1), min(R, n), d_at, root_true_delta,
                              root_prefix, pn, l8, r8, lcs, par,
                              EDGES ? edge_count + sb : nullptr);
+  }
+  __syncthreads();
+
+  // phase D: the tile's gaps whose nearest smaller gap lies beyond the
+  // window, one warp per gap (the warp-cooperative search of the keys in
+  // global memory); their latency overlaps the other resident blocks' work
+  const uint32_t nf = min(s_far_n, kTreeFarPerTile);
+  auto d_glob = [&](int p) -> int { return delta(codes[p], codes[p + 1]); };
+  for (uint32_t f = warp; f < nf; f += NW) {
+    const int g = int(s_far[f]);
+    const int D = delta(codes[g], codes[g + 1]);
+    int first_key, last_key;
+    coop_node_keys<K>(codes, n, g, D, &first_key, &last_key);
+    if (lane == 0)
+      write_gap_node<K, EDGES>(g, n, D, first_key - 1, last_key, d_glob, root_true_delta,
+                               root_prefix, pn, l8, r8, lcs, par,
+                               EDGES ? edge_count + sb : nullptr);
   }
 }
 
