@@ -46,7 +46,7 @@ def parse_args():
     p.add_argument("--n", type=int, default=16777216)
     p.add_argument("--dist", choices=("uniform", "gauss", "appdata"), default="uniform")
     p.add_argument("--key-bits", type=int, default=32, choices=(32, 64))
-    p.add_argument("--radix-bits", type=int, default=0, choices=(0, 8, 11))
+    p.add_argument("--radix-bits", type=int, default=0, choices=(0, 8, 10, 11))
     p.add_argument("--seed", type=int, default=20260101)
     p.add_argument("--no-verify", action="store_true", help="skip the oracle check")
     p.add_argument("--no-cpu-baseline", action="store_true")

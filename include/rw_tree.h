@@ -101,7 +101,7 @@ void rw_tree_app_data_init(rw_tree_app_data* app, uint32_t n_input,
  * scratch for up to n_input points on the current device. */
 int rw_tree_im_storage_create(uint32_t n_input, int32_t key_bits,
                               rw_tree_im_storage** out);
-/* Same, with the sort's digit width chosen: 8 or 11 bits (0 = default 8).
+/* Same, with the sort's digit width chosen: 8, 10 or 11 bits (0 = default 8).
  * The reference fixes 8-bit digits (cu_dispatcher.cu:25-27). */
 int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
                                  int32_t radix_bits, rw_tree_im_storage** out);

@@ -62,7 +62,7 @@ def time_batch(batch, reps: int) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def tune(rw, key_bits: int = 32, bounds=DEFAULT_BOUNDS, digit_widths=(8, 11),
+def tune(rw, key_bits: int = 32, bounds=DEFAULT_BOUNDS, digit_widths=(8, 10, 11),
          points_per_class: int = 6_000_000, reps: int = 5, seed: int = 1, log=print) -> dict:
     lows = [CLOUD_RANGE[0]] + [b + 1 for b in bounds]
     highs = list(bounds) + [CLOUD_RANGE[1]]

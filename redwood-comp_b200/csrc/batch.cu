@@ -217,7 +217,7 @@ extern "C" {
 int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t key_bits,
                          int32_t radix_bits, float octree_ratio, rw_tree_batch** out) {
   if (!out || !cloud_sizes || n_clouds < 1 || (key_bits != 32 && key_bits != 64) ||
-      (radix_bits != 0 && radix_bits != 8 && radix_bits != 11) || !(octree_ratio < 64.0f))
+      (radix_bits != 0 && radix_bits != 8 && radix_bits != 10 && radix_bits != 11) || !(octree_ratio < 64.0f))
     return RW_ERR_ARG;
   const float ratio = octree_ratio > 0.0f ? octree_ratio : 0.6f;
   *out = nullptr;

@@ -208,7 +208,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
                                  int32_t radix_bits, rw_tree_im_storage** out) {
   if (!out || n_input < 1 || n_input >= RW_MAX_POINTS ||
       (key_bits != 32 && key_bits != 64) ||
-      (radix_bits != 0 && radix_bits != 8 && radix_bits != 11))
+      (radix_bits != 0 && radix_bits != 8 && radix_bits != 10 && radix_bits != 11))
     return RW_ERR_ARG;
   *out = nullptr;
   int dev_count = 0;

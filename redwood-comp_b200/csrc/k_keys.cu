@@ -13,7 +13,7 @@
 // per-warp stable ranking (shared-memory atomic-OR peer masks by default;
 // ballot multi-split and match.any in the variant menu), the tile reordered by
 // digit in shared memory, and a per-digit decoupled look-back.  Digit width is
-// 8 or 11 bits; 32-bit keys take 4 or 3 passes, 64-bit keys 8 or 6.  The
+// 8, 10 or 11 bits; 32-bit keys take 4, 3 or 3 passes, 64-bit keys 8, 7 or 6.  The
 // default 32-bit variant (384 threads x 24 keys) runs three blocks per SM.
 #include <algorithm>
 
@@ -502,6 +502,13 @@ const SortVariant kVariants[] = {
     {32, 8, 512, 16, kRankMatchAny, passes_t<uint32_t, 8, 512, 16, kRankMatchAny, 2>},
     {32, 8, 1024, 16, kRankAtomicOr, passes_t<uint32_t, 8, 1024, 16, kRankAtomicOr, 1>},
     {32, 8, 1024, 8, kRankAtomicOr, passes_t<uint32_t, 8, 1024, 8, kRankAtomicOr, 1>},
+    {32, 10, 256, 24, kRankAtomicOr, passes_t<uint32_t, 10, 256, 24, kRankAtomicOr, 2>},
+    {32, 10, 256, 16, kRankAtomicOr, passes_t<uint32_t, 10, 256, 16, kRankAtomicOr, 2>},
+    {32, 10, 256, 24, kRankBallot, passes_t<uint32_t, 10, 256, 24, kRankBallot, 3>},
+    {32, 10, 384, 16, kRankBallot, passes_t<uint32_t, 10, 384, 16, kRankBallot, 2>},
+    {32, 10, 512, 16, kRankBallot, passes_t<uint32_t, 10, 512, 16, kRankBallot, 2>},
+    {32, 10, 256, 24, kRankMatchAny, passes_t<uint32_t, 10, 256, 24, kRankMatchAny, 3>},
+    {32, 10, 256, 24, kRankHalfPacked, passes_t<uint32_t, 10, 256, 24, kRankHalfPacked, 2>},
     {32, 11, 512, 16, kRankBallot, passes_t<uint32_t, 11, 512, 16, kRankBallot, 1>},
     {32, 11, 256, 16, kRankAtomicOr, passes_t<uint32_t, 11, 256, 16, kRankAtomicOr, 1>},
     {32, 11, 256, 24, kRankAtomicOr, passes_t<uint32_t, 11, 256, 24, kRankAtomicOr, 1>},
@@ -514,6 +521,8 @@ const SortVariant kVariants[] = {
     {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},
     {64, 8, 256, 12, kRankAtomicOr, passes_t<uint64_t, 8, 256, 12, kRankAtomicOr, 3>},
     {64, 8, 256, 16, kRankBallot, passes_t<uint64_t, 8, 256, 16, kRankBallot, 2>},
+    {64, 10, 256, 16, kRankAtomicOr, passes_t<uint64_t, 10, 256, 16, kRankAtomicOr, 2>},
+    {64, 10, 256, 16, kRankBallot, passes_t<uint64_t, 10, 256, 16, kRankBallot, 2>},
     {64, 11, 384, 16, kRankBallot, passes_t<uint64_t, 11, 384, 16, kRankBallot, 1>},
     {64, 11, 256, 16, kRankAtomicOr, passes_t<uint64_t, 11, 256, 16, kRankAtomicOr, 1>},
     {64, 11, 256, 12, kRankAtomicOr, passes_t<uint64_t, 11, 256, 12, kRankAtomicOr, 1>},
@@ -559,11 +568,14 @@ int default_sort_variant(int key_bits, int radix_bits) {
 
 cudaError_t launch_keys(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode,
                         bool hist, cudaStream_t s) {
-  if (b.key_bits == 32)
-    return sc.radix_bits == 8 ? keys_t<uint32_t, 8>(b, sc, pl, encode, hist, s)
-                              : keys_t<uint32_t, 11>(b, sc, pl, encode, hist, s);
-  return sc.radix_bits == 8 ? keys_t<uint64_t, 8>(b, sc, pl, encode, hist, s)
-                            : keys_t<uint64_t, 11>(b, sc, pl, encode, hist, s);
+  if (b.key_bits == 32) {
+    if (sc.radix_bits == 8) return keys_t<uint32_t, 8>(b, sc, pl, encode, hist, s);
+    if (sc.radix_bits == 10) return keys_t<uint32_t, 10>(b, sc, pl, encode, hist, s);
+    return keys_t<uint32_t, 11>(b, sc, pl, encode, hist, s);
+  }
+  if (sc.radix_bits == 8) return keys_t<uint64_t, 8>(b, sc, pl, encode, hist, s);
+  if (sc.radix_bits == 10) return keys_t<uint64_t, 10>(b, sc, pl, encode, hist, s);
+  return keys_t<uint64_t, 11>(b, sc, pl, encode, hist, s);
 }
 
 cudaError_t launch_sort_passes(const Bufs& b, const Scratch& sc, const Plan& pl,

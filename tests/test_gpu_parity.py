@@ -81,7 +81,8 @@ SIZES = (3, 31, 32, 33, 255, 256, 257, 1023, 1024, 1025, 4095, 4096, 4097,
          6143, 6144, 6145, 8191, 8192, 8193, 65537)
 
 
-@pytest.mark.parametrize("key_bits,radix_bits", [(32, 8), (32, 11), (64, 8), (64, 11)])
+@pytest.mark.parametrize("key_bits,radix_bits", [(32, 8), (32, 10), (32, 11), (64, 8),
+                                               (64, 10), (64, 11)])
 def test_ragged_sizes(rw, oracle, key_bits, radix_bits):
     for i, n in enumerate(SIZES):
         for kind in ("uniform", "gauss"):
