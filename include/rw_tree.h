@@ -368,7 +368,9 @@ typedef struct rw_tree_learned_stats {
   uint32_t max_bucket;  /* keys in the fullest bucket */
   uint32_t big_buckets; /* buckets above one CTA's 32,768 keys (chunked path) */
   uint32_t fell_back;   /* 1 when a bucket overflowed and the onesweep sort ran */
-  uint32_t reserved;
+  uint32_t mlp_timeout; /* 1 once a wait of the boundary network on the tensor cores
+                           ran out (sticky for this scratch; the boundaries of that
+                           tile stayed sample quantiles, the sort stays exact) */
 } rw_tree_learned_stats;
 
 /* Scratch for inputs of up to n_max (>= 65536) keys on the current device

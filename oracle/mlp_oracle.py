@@ -1,7 +1,8 @@
 """Test infrastructure: CPU (numpy, float32) restatement of the boundary MLP of
 the learned-CDF sort, forward and backward, to check the GPU training kernels'
-gradients.  Weights are rounded to BF16 (round to nearest, ties to even)
-before use, as the kernels do; biases and all arithmetic stay float32.
+gradients, and the tensor-core inference numerics (forward_inference).
+Weights are rounded to BF16 (round to nearest, ties to even) before use, as
+the kernels do; in training the biases and all arithmetic stay float32.
 
 Layout of the parameter vector: W1 [64][16], b1 [64], W2 [64][64], b2 [64],
 W3 [64], b3 [1].
@@ -37,6 +38,24 @@ def forward(p: np.ndarray, x: np.ndarray) -> np.ndarray:
     h1 = np.maximum(x @ w1.T + q["b1"], 0).astype(np.float32)
     h2 = np.maximum(h1 @ w2.T + q["b2"], 0).astype(np.float32)
     return (h2 @ w3 + q["b3"][0]).astype(np.float32)
+
+
+def forward_inference(p: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """The inference numerics of the tensor-core kernels: inputs, W1, W2 and
+    the hidden activations of layer 1 rounded to BF16, the two hidden layers'
+    products summed exactly (float64, then float32) before the float32 bias,
+    ReLU; the output b3 + sum_u w3[u] h2[u] in float32, units in order."""
+    q = unpack(np.asarray(p, np.float32))
+    w1, w2, w3 = bf16_round(q["w1"]), bf16_round(q["w2"]), bf16_round(q["w3"])
+    xb = bf16_round(np.asarray(x, np.float32)).astype(np.float64)
+    z1 = (xb @ w1.T.astype(np.float64)).astype(np.float32) + q["b1"]
+    h1 = bf16_round(np.maximum(z1, 0).astype(np.float32)).astype(np.float64)
+    z2 = (h1 @ w2.T.astype(np.float64)).astype(np.float32) + q["b2"]
+    h2 = np.maximum(z2, 0).astype(np.float32)
+    y = np.full(len(xb), q["b3"][0], np.float32)
+    for u in range(H):
+        y = (y + w3[u] * h2[:, u]).astype(np.float32)
+    return y
 
 
 def grad(p: np.ndarray, x: np.ndarray, t: np.ndarray, batch: int):

@@ -214,7 +214,7 @@ class ImStorage:
         st = _LearnedStatsC()
         _check(lib().rw_tree_im_storage_learned_stats(self._h, ctypes.byref(st)), "learned_stats")
         return {"max_bucket": st.max_bucket, "big_buckets": st.big_buckets,
-                "fell_back": st.fell_back}
+                "fell_back": st.fell_back, "mlp_timeout": st.mlp_timeout}
 
     def clear(self, stream=None) -> None:
         _check(lib().rw_tree_im_storage_clear(self._h, _stream_handle(stream)), "clearSmem")
@@ -619,7 +619,7 @@ MLP_PARAMS = 5313
 
 class _LearnedStatsC(ctypes.Structure):
     _fields_ = [("max_bucket", ctypes.c_uint32), ("big_buckets", ctypes.c_uint32),
-                ("fell_back", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("fell_back", ctypes.c_uint32), ("mlp_timeout", ctypes.c_uint32)]
 
 
 def _dptr(t) -> _vp:
@@ -672,7 +672,7 @@ class Learned:
                                           ctypes.c_int32(mode), im, _stream_handle(stream),
                                           ctypes.byref(st)), "learned_sort")
         return out, {"max_bucket": st.max_bucket, "big_buckets": st.big_buckets,
-                     "fell_back": st.fell_back}
+                     "fell_back": st.fell_back, "mlp_timeout": st.mlp_timeout}
 
     def features(self, keys, stream=None):
         """(MLP inputs [4095, 16] under the current group size, sorted sample

@@ -44,6 +44,7 @@
 #include <vector>
 
 #include "internal.hpp"
+#include "mlp.cuh"
 #include "rank.cuh"
 
 namespace rwt {
@@ -75,7 +76,7 @@ struct LearnedPlan {
   uint32_t max_count;
   uint32_t n_big;       // buckets above kBucketCap
   uint32_t fallback;    // some bucket overflowed its region
-  uint32_t pad;
+  uint32_t mlp_timeout; // copy of the boundary network's error word
 };
 
 __device__ __forceinline__ uint32_t mix32(uint32_t x) {
@@ -226,63 +227,32 @@ __device__ __forceinline__ uint32_t bucket_of(const uint32_t* s_t, uint32_t k) {
   return i - kBuckets;
 }
 
-// 2'. MLP boundaries, evaluated in parallel: 64 threads per boundary (one
-// hidden unit each), four boundaries per round, kBpRounds rounds per CTA.
-// The inputs are those k_boundaries writes for training.
-constexpr int kBpThreads = 256, kBpGroup = kBpThreads / kMlpHidden, kBpRounds = 1;
-constexpr uint32_t kBpPerCta = kBpGroup * kBpRounds;
-
-__global__ void __launch_bounds__(kBpThreads)
+// 2'. MLP boundaries on the tensor cores: one CTA per 128 boundaries, thread
+// t computes boundary (CTA * 128 + t)'s inputs (those k_boundaries writes for
+// training), the two hidden layers are tcgen05 MMAs (mlp.cuh), and the thread
+// turns its row's output into the boundary key.  A boundary whose context does
+// not fit inside the sample, or whose CTA's tensor-core wait ran out (*err set),
+// stays the sample quantile.
+__global__ void __launch_bounds__(kMlpTcThreads)
     k_boundaries_mlp(const uint32_t* __restrict__ sorted_sample, const float* __restrict__ params,
-                     uint32_t group, uint32_t* __restrict__ bounds) {
+                     uint32_t group, uint32_t* __restrict__ bounds, uint32_t* __restrict__ err) {
   pdl_enter();
-  __shared__ float s_w1[kMlpHidden * kMlpIn], s_w2[kMlpHidden * kMlpHidden], s_w3[kMlpHidden],
-      s_b1[kMlpHidden], s_b2[kMlpHidden];
-  __shared__ float s_x[kBpGroup][kMlpIn], s_h1[kBpGroup][kMlpHidden], s_part[kBpGroup][2];
-  constexpr int oW1 = 0, oB1 = oW1 + kMlpHidden * kMlpIn, oW2 = oB1 + kMlpHidden,
-                oB2 = oW2 + kMlpHidden * kMlpHidden, oW3 = oB2 + kMlpHidden;
-  for (int i = threadIdx.x; i < kMlpHidden * kMlpIn; i += kBpThreads)
-    s_w1[i] = __bfloat162float(__float2bfloat16_rn(params[oW1 + i]));
-  for (int i = threadIdx.x; i < kMlpHidden * kMlpHidden; i += kBpThreads)
-    s_w2[i] = __bfloat162float(__float2bfloat16_rn(params[oW2 + i]));
-  for (int i = threadIdx.x; i < kMlpHidden; i += kBpThreads) {
-    s_w3[i] = __bfloat162float(__float2bfloat16_rn(params[oW3 + i]));
-    s_b1[i] = params[oB1 + i];
-    s_b2[i] = params[oB2 + i];
-  }
-  const float b3 = params[kMlpParams - 1];
-  const int g = threadIdx.x / kMlpHidden, u = threadIdx.x % kMlpHidden;
   const uint32_t half = (kMlpIn / 2) * group;
-  for (int r = 0; r < kBpRounds; ++r) {
-    const uint32_t j = (blockIdx.x * kBpRounds + r) * kBpGroup + g;
-    const uint32_t c = (j + 1) * kSpacing;
-    const bool live = j < kBounds;
-    const bool fits = live && c >= half && c + half <= kSample;
-    __syncthreads();  // weights loaded; the previous round's s_x / s_h1 read
-    if (fits && u < kMlpIn) s_x[g][u] = boundary_feature(sorted_sample, c, half, group, u);
-    __syncthreads();
-    if (fits) {
-      float acc = s_b1[u];
-#pragma unroll
-      for (int k = 0; k < kMlpIn; ++k) acc = fmaf(s_w1[u * kMlpIn + k], s_x[g][k], acc);
-      s_h1[g][u] = fmaxf(acc, 0.0f);
-    }
-    __syncthreads();
-    float part = 0.0f;
-    if (fits) {
-      float acc = s_b2[u];
-#pragma unroll 16
-      for (int k = 0; k < kMlpHidden; ++k) acc = fmaf(s_w2[u * kMlpHidden + k], s_h1[g][k], acc);
-      part = s_w3[u] * fmaxf(acc, 0.0f);
-    }
-    part = warp_sum(part);
-    if ((threadIdx.x & 31) == 0) s_part[g][(threadIdx.x >> 5) & 1] = part;
-    __syncthreads();
-    if (u == 0 && live)
-      bounds[j] = fits ? boundary_from_output(sorted_sample, c, half,
-                                              b3 + s_part[g][0] + s_part[g][1])
-                       : sorted_sample[c];
-  }
+  const uint32_t j = blockIdx.x * uint32_t(kMlpTcRows) + threadIdx.x;
+  const uint32_t c = (j + 1) * kSpacing;  // sample rank of the ideal boundary
+  const bool fits = j < kBounds && c >= half && c + half <= kSample;
+  mlp_tile_tc(
+      params,
+      [&](int, float (&x)[kMlpIn]) {
+        if (fits) boundary_features(sorted_sample, c, half, group, x);
+        return fits;
+      },
+      [&](int, float y, bool ok) {
+        if (j < kBounds)
+          bounds[j] = fits && ok ? boundary_from_output(sorted_sample, c, half, y)
+                                 : sorted_sample[c];
+      },
+      err);
 }
 
 // 4. one split pass.  Segment `seg` of the source (its keys: n, or
@@ -417,8 +387,9 @@ __global__ void __launch_bounds__(1024)
     k_bucket_plan(const uint32_t* __restrict__ counts, uint32_t cap,
                   const uint32_t* __restrict__ super_counts, uint32_t scap,
                   uint32_t* __restrict__ offsets, uint32_t* __restrict__ order,
-                  LearnedPlan* __restrict__ plan) {
+                  LearnedPlan* __restrict__ plan, const uint32_t* __restrict__ mlp_err) {
   pdl_enter();
+  if (threadIdx.x == 0) plan->mlp_timeout = *mlp_err;
   __shared__ uint32_t s_warp[33];
   __shared__ uint32_t s_front, s_back;
   constexpr int R = kBuckets / 1024;
@@ -748,6 +719,7 @@ struct rw_tree_learned {
   float* d_features = nullptr;
   rwt::LearnedPlan* d_plan = nullptr;
   rwt::LearnedPlan* h_plan = nullptr;
+  uint32_t* d_mlp_err = nullptr;  // set when a boundary network wait ran out (sticky)
   uint32_t group = 4;  // sample keys per MLP input
   bool has_params = false;
 };
@@ -783,9 +755,9 @@ int boundaries(rw_tree_learned* L, bool mlp, bool features, cudaStream_t s) {
     RWL_CUDA(cudaGetLastError());
   }
   if (mlp) {
-    const uint32_t ctas = (rwt::kBounds + rwt::kBpPerCta - 1) / rwt::kBpPerCta;
-    rwt::launch_pdl(rwt::k_boundaries_mlp, ctas, rwt::kBpThreads, 0, s, L->d_sample_sorted, L->d_params,
-                                                          L->group, L->d_bounds);
+    const uint32_t ctas = (rwt::kBounds + rwt::kMlpTcRows - 1) / rwt::kMlpTcRows;
+    rwt::launch_pdl(rwt::k_boundaries_mlp, ctas, rwt::kMlpTcThreads, 0, s, L->d_sample_sorted,
+                    L->d_params, L->group, L->d_bounds, L->d_mlp_err);
     RWL_CUDA(cudaGetLastError());
     rwt::launch_pdl(rwt::k_bounds_monotone, 1, 1024, 0, s, L->d_bounds);
   } else if (!features) {
@@ -821,7 +793,7 @@ int scatter_and_plan(rw_tree_learned* L, const uint32_t* keys, uint32_t n, cudaS
       L->d_region, cap);
   RWL_CUDA(cudaGetLastError());
   rwt::launch_pdl(rwt::k_bucket_plan, 1, 1024, 0, s, L->d_cursor, cap, L->d_super_cursor, scap, L->d_offsets,
-                                        L->d_order, L->d_plan);
+                                        L->d_order, L->d_plan, L->d_mlp_err);
   RWL_CUDA(cudaGetLastError());
   RWL_CUDA(cudaMemcpyAsync(L->h_plan, L->d_plan, sizeof(rwt::LearnedPlan),
                            cudaMemcpyDeviceToHost, s));
@@ -860,6 +832,7 @@ void learned_last_stats(const rw_tree_learned* L, rw_tree_learned_stats* out) {
   out->max_bucket = L->h_plan->max_count;
   out->big_buckets = L->h_plan->n_big;
   out->fell_back = L->h_plan->fallback;
+  out->mlp_timeout = L->h_plan->mlp_timeout;
 }
 
 }  // namespace rwt
@@ -883,10 +856,11 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
   auto up = [](size_t words) { return (words + 63) & ~size_t(63); };  // 256-byte pieces
   const size_t w_sample = up(rwt::kSample), w_b = up(rwt::kBuckets + 1),
                w_params = up(rwt::kMlpParams), w_feat = up(size_t(rwt::kBounds) * rwt::kMlpIn),
-               w_plan = up(sizeof(rwt::LearnedPlan) / 4),
+               w_plan = up(sizeof(rwt::LearnedPlan) / 4), w_err = up(1),
                w_region = size_t(rwt::kBuckets) * L->cap_max,
                w_super = size_t(rwt::kSupers) * L->scap_max;
-  const size_t words = 2 * w_sample + 5 * w_b + w_params + w_feat + w_plan + w_region + w_super;
+  const size_t words =
+      2 * w_sample + 5 * w_b + w_params + w_feat + w_plan + w_err + w_region + w_super;
   cudaError_t e = cudaMalloc(&L->d_mem, 4 * words);
   if (e == cudaSuccess) e = cudaMallocHost(&L->h_plan, sizeof(rwt::LearnedPlan));
   if (e != cudaSuccess) {
@@ -904,8 +878,14 @@ int rw_tree_learned_create(uint32_t n_max, rw_tree_learned** out) {
   L->d_params = reinterpret_cast<float*>(p); p += w_params;
   L->d_features = reinterpret_cast<float*>(p); p += w_feat;
   L->d_plan = reinterpret_cast<rwt::LearnedPlan*>(p); p += w_plan;
+  L->d_mlp_err = p; p += w_err;
   L->d_region = p; p += w_region;
   L->d_super_region = p;
+  e = cudaMemset(L->d_mlp_err, 0, 4);
+  if (e != cudaSuccess) {
+    rw_tree_learned_destroy(L);
+    return lfail(e, "rw_tree_learned_create");
+  }
   cudaFuncSetAttribute(rwt::k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        int(rwt::kBsSmem));
   *out = L;

@@ -1,9 +1,11 @@
 // The boundary MLP of the learned-CDF sort: 16 -> 64 -> 64 -> 1, ReLU,
 // BF16 weights with FP32 master copies, FP32 biases and FP32 accumulation.
-// Forward, backward and Adam are hand-written: a block takes 32 rows and runs
-// the layers as small matrix products in shared memory; weight gradients are
-// reduced per block and added to the global gradient once.  No reference
-// counterpart (the reference has no learned component).
+// Training (forward + backward, FP32 activations) and Adam are hand-written
+// for the CUDA cores: a block takes 32 rows and runs the layers as small
+// matrix products in shared memory; weight gradients are reduced per block and
+// added to the global gradient once.  Inference runs on the tensor cores
+// (mlp.cuh).  No reference counterpart (the reference has no learned
+// component).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -152,22 +154,33 @@ __global__ void k_adam(float* __restrict__ params, const float* __restrict__ gra
   params[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 }
 
-// Forward only (inference on `rows` feature rows), weights in BF16.
-__global__ void __launch_bounds__(kMlpThreads)
+// Forward only (inference on `rows` feature rows) on the tensor cores, 128
+// rows per CTA (mlp.cuh); a row whose tensor-core wait ran out gets NaN.
+__global__ void __launch_bounds__(kMlpTcThreads)
     k_mlp_forward(const float* __restrict__ params, const float* __restrict__ x, uint32_t rows,
                   float* __restrict__ y) {
-  __shared__ float s_w1[kH * kIn], s_w2[kH * kH], s_w3[kH], s_b1[kH], s_b2[kH];
-  for (int i = threadIdx.x; i < kH * kIn; i += kMlpThreads) s_w1[i] = bf16_round(params[kOffW1 + i]);
-  for (int i = threadIdx.x; i < kH * kH; i += kMlpThreads) s_w2[i] = bf16_round(params[kOffW2 + i]);
-  for (int i = threadIdx.x; i < kH; i += kMlpThreads) {
-    s_w3[i] = bf16_round(params[kOffW3 + i]);
-    s_b1[i] = params[kOffB1 + i];
-    s_b2[i] = params[kOffB2 + i];
-  }
-  __syncthreads();
-  const uint32_t row = blockIdx.x * kMlpThreads + threadIdx.x;
-  if (row >= rows) return;
-  y[row] = mlp_eval(x + size_t(row) * kIn, s_w1, s_b1, s_w2, s_b2, s_w3, params[kOffB3]);
+  const uint32_t r0 = blockIdx.x * uint32_t(kMlpTcRows);
+  mlp_tile_tc(
+      params,
+      [&](int t, float (&v)[kMlpIn]) {
+        const uint32_t row = r0 + uint32_t(t);
+        if (row >= rows) return false;
+        const float4* src = reinterpret_cast<const float4*>(x + size_t(row) * kMlpIn);
+#pragma unroll
+        for (int q = 0; q < kMlpIn / 4; ++q) {
+          const float4 f = src[q];
+          v[4 * q] = f.x;
+          v[4 * q + 1] = f.y;
+          v[4 * q + 2] = f.z;
+          v[4 * q + 3] = f.w;
+        }
+        return true;
+      },
+      [&](int t, float out, bool ok) {
+        const uint32_t row = r0 + uint32_t(t);
+        if (row < rows) y[row] = ok ? out : __int_as_float(0x7fc00000);
+      },
+      nullptr);
 }
 
 }  // namespace rwt
@@ -199,7 +212,8 @@ int rw_tree_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_
 int rw_tree_mlp_forward(const float* d_params, const float* d_x, uint32_t rows, float* d_y,
                         rw_stream_t stream) {
   if (!d_params || !d_x || !d_y || rows < 1) return RW_ERR_ARG;
-  rwt::k_mlp_forward<<<(rows + rwt::kMlpThreads - 1) / rwt::kMlpThreads, rwt::kMlpThreads, 0,
+  if (reinterpret_cast<uintptr_t>(d_x) & 15u) return RW_ERR_ARG;  // rows are read as float4
+  rwt::k_mlp_forward<<<(rows + rwt::kMlpTcRows - 1) / rwt::kMlpTcRows, rwt::kMlpTcThreads, 0,
                        reinterpret_cast<cudaStream_t>(stream)>>>(d_params, d_x, rows, d_y);
   return cudaGetLastError() == cudaSuccess ? RW_OK : RW_ERR_CUDA;
 }

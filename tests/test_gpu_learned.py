@@ -26,7 +26,16 @@ def test_mlp_forward_and_grad_match_cpu_oracle(rw):
     t = rng.random(rows, dtype=np.float32)
     dp, dx, dt = (torch.from_numpy(a).cuda() for a in (p, x, t))
     y = rw.mlp_forward(dp, dx).cpu().numpy()
-    np.testing.assert_allclose(y, mlp_oracle.forward(p, x), rtol=1e-5, atol=1e-5)
+    want_y = mlp_oracle.forward_inference(p, x)
+    # the tensor cores sum the products in FP32 in their own order; a hidden
+    # value that lands next to a BF16 rounding midpoint may round the other
+    # way (one BF16 step, 2^-8 relative), so a few rows move by ~1e-4
+    err = np.abs(y - want_y)
+    assert np.median(err) <= 2e-6 * max(1.0, float(np.abs(want_y).max())), np.median(err)
+    np.testing.assert_allclose(y, want_y, rtol=2e-3, atol=2e-3)
+    # and the network is the training network: FP32 activations agree to the
+    # precision of BF16 activations
+    np.testing.assert_allclose(y, mlp_oracle.forward(p, x), rtol=1e-2, atol=1e-2)
     g, loss = rw.mlp_grad(dp, dx, dt, rows)
     want, want_loss = mlp_oracle.grad(p, x, t, rows)
     # float32 sums in a different order: relative 1e-4 of the largest entry
