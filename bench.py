@@ -613,6 +613,41 @@ def ref_cuda_isolated(a, warmup=2, iters=10):
     return out
 
 
+def copy_floor_ms(app, h_pts, outs, m, reps):
+    """Device time of one step's host copies alone: the points host to device
+    on one stream while the five octree arrays (m rows) go device to host on
+    another, from and to the same pinned buffers the end-to-end step uses."""
+    import torch
+    pairs = [(outs["children"][:m], app.oct_children[:m]), (outs["corner"][:m], app.oct_corner[:m]),
+             (outs["cell_size"][:m], app.oct_cell_size[:m]),
+             (outs["child_node_mask"][:m], app.oct_child_node_mask[:m]),
+             (outs["child_leaf_mask"][:m], app.oct_child_leaf_mask[:m])]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def step():
+        with torch.cuda.stream(s_in):
+            app.u_input_points.copy_(h_pts, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            for h, d in pairs:
+                h.copy_(d, non_blocking=True)
+
+    cur = torch.cuda.current_stream()
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    s_in.wait_stream(cur)
+    s_out.wait_stream(cur)
+    for _ in range(reps):
+        step()
+    cur.wait_stream(s_in)
+    cur.wait_stream(s_out)
+    e1.record(cur)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def rank_barrier(world):
     """Every rank waits for the others (the timed regions start and end
     together); nothing with one process."""
@@ -832,10 +867,15 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
     m2 = app.get_n_octree_nodes()
     d2h = 60 * m2 + 16
+    floor_ms = copy_floor_ms(app, h_pts, outs, m2, e2e_steps)
     e2e = {"value": a.n * world / (e2e_ms / 1e3), "unit": "points/s",
            "h2d_bytes_per_step": 16 * a.n, "d2h_bytes_per_step": d2h,
            "ms_per_step": round(e2e_ms, 4),
            "single_slot_ms_per_step": round(single_ms, 4),
+           "copy_floor_ms": round(floor_ms, 4),
+           "copy_floor_note": "the same step's copies alone (points host to device on one "
+                              "stream, the five octree arrays device to host on another, "
+                              "pinned buffers, no kernels), the PCIe bound of this number",
            "path": "rw_tree_host_submit / rw_tree_host_collect on three AppData/scratch "
                    "pairs and three streams: pinned host points -> H2D -> 7 stages -> counts + "
                    "octree rows (children, corner, cell_size, masks) D2H, every step"}

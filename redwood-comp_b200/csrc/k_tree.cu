@@ -10,7 +10,8 @@
 // func_brt.hpp:45-138) from nearest smaller values: the radix tree is the
 // Cartesian tree of the gap deltas, so each gap's node follows from the
 // nearest strictly smaller gap on either side (k_radix_tree; the few gaps
-// whose answer lies beyond the tile's window go to k_radix_tree_far).  Node 0
+// whose answer lies beyond the tile's window are searched for in the keys by
+// the block at its end).  Node 0
 // keeps the reference's own search over [0, n_brt-1] (brt_node, write_node);
 // nodes i >= 1 are the true Karras nodes and each names its children once, so
 // the parent writes are deterministic.
@@ -417,8 +418,9 @@ struct GlobalKeys {
 // tile and a halo of kAnsvHalo chunks on either side, per-value bitmasks of
 // the chunks whose minimum lies below v find the nearest such chunk in one
 // clz / ffs, and its summary gives the answer; a gap whose nearest smaller
-// lies beyond the halo (a node near the top of the tree) goes to a list that a
-// second kernel resolves with warp-cooperative searches of the keys.
+// lies beyond the halo (a node near the top of the tree) goes to a list in
+// shared memory that the block resolves at its end with warp-cooperative
+// searches of the keys.
 constexpr int kAnsvHalo = 8;                                        // chunks per side
 constexpr int kAnsvChunks = int(kTreeTile) / 32 + 2 * kAnsvHalo;   // chunks per window
 constexpr int kAnsvWin = kAnsvChunks * 32;                           // gaps per window
@@ -522,11 +524,11 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
                  const uint32_t* __restrict__ n_unique, int32_t* __restrict__ seg_err,
                  uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
                  uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
-                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count,
-                 uint32_t* __restrict__ far, uint32_t far_cap, uint32_t* __restrict__ far_n) {
+                 int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
   pdl_enter();
   using C = AnsvCfg<K>;
   constexpr int NV = C::NV, VB = C::VB, NW = kTreeThreads / 32;
+  static_assert(kTreeFarPerTile >= 2 * uint32_t(NV), "far gaps of a tile: NV per side");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // positions inside a chunk are kept as lane indices (0xff: none)
   K* s_key = reinterpret_cast<K*>(smem_raw);                                   // [kAnsvWin + 1]
@@ -721,18 +723,15 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       }
     }
     if (L == kAnsvNone || R == kAnsvNoneR) {
-      // resolved by this block below (at most kTreeFarPerTile per tile); the
-      // global list and k_radix_tree_far only if that ever overflowed
+      // resolved by this block below.  The list cannot overflow: two gaps
+      // whose nearest smaller gap on the left lies beyond the window never
+      // share a value (if a < b did, every gap between them would be at least
+      // that value, so the keys a+1 .. b would all have the bit at which keys
+      // a and a+1 first differ set, while gap b needs key b to have it clear),
+      // so the tile holds at most NV such gaps, and NV more on the right
       const uint32_t local = atomicAdd(&s_far_n, 1u);
-      if (local < kTreeFarPerTile) {
-        s_far[local] = uint32_t(g);
-        continue;
-      }
-      const uint32_t slot = atomicAdd(far_n, 1u);
-      if (slot < far_cap) {
-        far[2 * slot] = sb + uint32_t(g);
-        far[2 * slot + 1] = c;
-      }
+      if (local < kTreeFarPerTile) s_far[local] = uint32_t(g);
+      else seg_error(seg_err, c, RW_ERR_CAPACITY);  // not reachable, see above
       continue;
     }
     write_gap_node<K, EDGES>(g, n, e - 1, max(L, -1), min(R, n), d_at, root_true_delta,
@@ -755,40 +754,6 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       write_gap_node<K, EDGES>(g, n, D, first_key - 1, last_key, d_glob, root_true_delta,
                                root_prefix, pn, l8, r8, lcs, par,
                                EDGES ? edge_count + sb : nullptr);
-  }
-}
-
-// The far-search list: one warp per listed gap finds both nearest smaller
-// gaps in global memory and writes the gap's node.
-template <typename K, bool EDGES>
-__global__ void __launch_bounds__(256)
-    k_radix_tree_far(const K* __restrict__ codes_all, SegTable seg,
-                     const uint32_t* __restrict__ n_unique, const uint32_t* __restrict__ far,
-                     const uint32_t* __restrict__ far_n, uint32_t far_cap,
-                     uint8_t* __restrict__ prefix_n, uint8_t* __restrict__ hl,
-                     uint8_t* __restrict__ hr, int32_t* __restrict__ lc,
-                     int32_t* __restrict__ parents, int32_t* __restrict__ edge_count) {
-  pdl_enter();
-  const uint32_t count = min(*far_n, far_cap);
-  const uint32_t warps = gridDim.x * (blockDim.x / 32);
-  for (uint32_t w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w < count; w += warps) {
-    const uint32_t c = far[2 * w + 1];
-    const uint32_t sb = seg_begin(seg, c);
-    const int n = int(n_unique[c]) - 1;
-    const int g = int(far[2 * w] - sb);
-    const K* codes = codes_all + sb;
-    const int D = delta(codes[g], codes[g + 1]);
-    int first_key, last_key;
-    coop_node_keys<K>(codes, n, g, D, &first_key, &last_key);
-    const int L = first_key - 1;
-    const int R = last_key;
-    if (lane_id() == 0) {
-      auto d_at = [&](int p) -> int { return delta(codes[p], codes[p + 1]); };
-      const int rtd = EDGES ? delta(codes[0], codes[n]) : 0;
-      const int rp = EDGES ? delta(codes[0], codes[n - 1]) : 0;
-      write_gap_node<K, EDGES>(g, n, D, L, R, d_at, rtd, rp, prefix_n + sb, hl + sb, hr + sb,
-                               lc + sb, parents + sb, EDGES ? edge_count + sb : nullptr);
-    }
   }
 }
 
@@ -1517,23 +1482,13 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
   cudaError_t e = cudaFuncSetAttribute(edges ? k_radix_tree<K, true> : k_radix_tree<K, false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  uint32_t* far_n = sc.tile_ctr + kCtrTree;
-  const int far_blocks = std::max(1, sc.num_sms * 8);
-  if (edges) {
-    launch_pdl(k_radix_tree<K, true>, tiles, kTreeThreads, smem, s, 
-        codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
-        b.parents, b.edge_count, sc.tree_far, sc.tree_far_cap, far_n);
-    launch_pdl(k_radix_tree_far<K, true>, far_blocks, 256, 0, s, 
-        codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
-        b.hr, b.lc, b.parents, b.edge_count);
-  } else {
-    launch_pdl(k_radix_tree<K, false>, tiles, kTreeThreads, smem, s, 
-        codes, pl.seg, pl.tree_map, pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc,
-        b.parents, nullptr, sc.tree_far, sc.tree_far_cap, far_n);
-    launch_pdl(k_radix_tree_far<K, false>, far_blocks, 256, 0, s, 
-        codes, pl.seg, pl.n_unique, sc.tree_far, far_n, sc.tree_far_cap, b.prefix_n, b.hl,
-        b.hr, b.lc, b.parents, nullptr);
-  }
+  if (edges)
+    launch_pdl(k_radix_tree<K, true>, tiles, kTreeThreads, smem, s, codes, pl.seg, pl.tree_map,
+               pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc, b.parents, b.edge_count);
+  else
+    launch_pdl(k_radix_tree<K, false>, tiles, kTreeThreads, smem, s, codes, pl.seg, pl.tree_map,
+               pl.n_unique, pl.seg_err, b.prefix_n, b.hl, b.hr, b.lc, b.parents,
+               static_cast<int32_t*>(nullptr));
   return cudaGetLastError();
 }
 
