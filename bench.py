@@ -34,6 +34,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "octree-build points/sec (7 stages, bit-exact): plain vs batched/learned, 1 B200"
+# warp ranking schemes of the onesweep variants (rw_tree_sort_variant_info rank_mode)
+RANK_NAMES = ("ballot", "match_any", "atomic_or", "half_packed", "atomic_or+ballot_top")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -336,7 +338,7 @@ def measure_batch(rw, a, n_clouds=1024, verify_clouds=96):
         "tuning": batch.tuning and {"radix_bits": batch.tuning["radix_bits"],
                                     "classes": [(c["max_points"],
                                                  f'{c["threads"]}x{c["keys_per_thread"]} '
-                                                 f'{("ballot", "match_any", "atomic_or")[c["rank"]]}')
+                                                 f'{RANK_NAMES[c["rank"]]}')
                                                 for c in batch.tuning["classes"]]},
         "graph": True,
     }

@@ -107,7 +107,8 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
                                  int32_t radix_bits, rw_tree_im_storage** out);
 /* The onesweep sort comes in a menu of variants (threads per CTA, keys per
  * thread, warp ranking scheme: 0 ballot multi-split, 1 match.any,
- * 2 shared-memory atomic OR) for each key and digit width; the autotuner
+ * 2 shared-memory atomic OR, 3 half-warp packed words, 4 atomic OR with the
+ * top pass by ballots over its remaining bits) for each key and digit width; the autotuner
  * picks one per size class.  No reference counterpart (the reference fixes
  * 512 threads x 15 keys with ballots, cu_dispatcher.cu:44-49). */
 int rw_tree_sort_variant_count(void);

@@ -51,7 +51,8 @@ struct rw_tree_batch {
   uint32_t tree_far_cap = 0;
   void* d_zero = nullptr;
   size_t zero_bytes = 0;
-  uint32_t *d_ghist = nullptr, *d_sort_desc = nullptr, *d_unique_desc = nullptr,
+  uint32_t *d_ghist = nullptr, *d_skew = nullptr, *d_sort_desc = nullptr,
+           *d_unique_desc = nullptr,
            *d_scan_desc = nullptr, *d_tile_ctr = nullptr;
   rwt::DevStatus* d_status = nullptr;
   uint32_t *d_n_unique = nullptr, *d_n_octree = nullptr;
@@ -155,6 +156,7 @@ rwt::Scratch scratch_of(const rw_tree_batch* b) {
   sc.passes = b->passes;
   sc.sort_variant = b->sort_variant;
   sc.ghist = b->d_ghist;
+  sc.skew = b->d_skew;
   sc.sort_desc = b->d_sort_desc;
   sc.sort_rows = b->sort_rows;
   sc.unique_desc = b->d_unique_desc;
@@ -280,7 +282,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
   const size_t per_b = align(size_t(n_clouds) * 4);
-  b->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b + 3 * per_b;
+  b->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b + 4 * per_b;
 
   const size_t ks = key_bits == 32 ? 4 : 8;
   cudaError_t e = cudaMalloc(&b->d_tables, (8 + rwt::kMaxSortClasses) * tab * 4);
@@ -314,6 +316,7 @@ int rw_tree_batch_create(const uint32_t* cloud_sizes, uint32_t n_clouds, int32_t
   b->d_n_unique = reinterpret_cast<uint32_t*>(z + o); o += per_b;
   b->d_n_octree = reinterpret_cast<uint32_t*>(z + o); o += per_b;
   b->d_seg_err = reinterpret_cast<int32_t*>(z + o); o += per_b;
+  b->d_skew = reinterpret_cast<uint32_t*>(z + o); o += per_b;
 
   std::vector<uint32_t> all;
   all.reserve(8 * tab);

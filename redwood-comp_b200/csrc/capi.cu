@@ -98,6 +98,7 @@ rwt::Scratch scratch_of(const rw_tree_im_storage* im) {
   sc.passes = im->passes;
   sc.sort_variant = im->sort_variant;
   sc.ghist = im->d_ghist;
+  sc.skew = im->d_skew;
   sc.sort_desc = im->d_sort_desc;
   sc.sort_rows = im->sort_tiles + 1;
   sc.unique_desc = im->d_unique_desc;
@@ -233,6 +234,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
 
   auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t ghist_b = align(size_t(im->passes) * radix * 4);
+  const size_t skew_b = align(4);
   const size_t sdesc_b = align(size_t(im->passes) * (im->sort_tiles + 1) * radix * 4);
   const size_t udesc_b = align((size_t(rwt::div_up(n_input, rwt::kUniqueTile)) + 1) * 4);
   // stage 6's tiles, or the octree's (smaller) ones in the fused pipeline
@@ -240,7 +242,7 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
   static_assert(rwt::kOctTile <= rwt::kScanTile, "scan descriptors sized by the octree tiles");
   const size_t ctr_b = align(rwt::kCounters * 4);
   const size_t st_b = align(sizeof(rwt::DevStatus));
-  im->zero_bytes = ghist_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b;
+  im->zero_bytes = ghist_b + skew_b + sdesc_b + udesc_b + cdesc_b + ctr_b + st_b;
 
   cudaError_t e = cudaMalloc(&im->d_zero, im->zero_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&im->d_tmp_keys, key_size(key_bits) * n_input);
@@ -252,13 +254,14 @@ int rw_tree_im_storage_create_ex(uint32_t n_input, int32_t key_bits,
     return cuda_fail(e, "rw_tree_im_storage_create");
   }
   char* z = static_cast<char*>(im->d_zero);
-  im->d_ghist = reinterpret_cast<uint32_t*>(z);
-  im->d_sort_desc = reinterpret_cast<uint32_t*>(z + ghist_b);
-  im->d_unique_desc = reinterpret_cast<uint32_t*>(z + ghist_b + sdesc_b);
-  im->d_scan_desc = reinterpret_cast<uint32_t*>(z + ghist_b + sdesc_b + udesc_b);
-  im->d_tile_ctr = reinterpret_cast<uint32_t*>(z + ghist_b + sdesc_b + udesc_b + cdesc_b);
-  im->d_status = reinterpret_cast<rwt::DevStatus*>(z + ghist_b + sdesc_b + udesc_b +
-                                                   cdesc_b + ctr_b);
+  size_t o = 0;
+  im->d_ghist = reinterpret_cast<uint32_t*>(z + o); o += ghist_b;
+  im->d_skew = reinterpret_cast<uint32_t*>(z + o); o += skew_b;
+  im->d_sort_desc = reinterpret_cast<uint32_t*>(z + o); o += sdesc_b;
+  im->d_unique_desc = reinterpret_cast<uint32_t*>(z + o); o += udesc_b;
+  im->d_scan_desc = reinterpret_cast<uint32_t*>(z + o); o += cdesc_b;
+  im->d_tile_ctr = reinterpret_cast<uint32_t*>(z + o); o += ctr_b;
+  im->d_status = reinterpret_cast<rwt::DevStatus*>(z + o);
   std::memset(im->h_status, 0, sizeof(rwt::DevStatus));
   e = cudaMemset(im->d_zero, 0, im->zero_bytes);
   if (e != cudaSuccess) {

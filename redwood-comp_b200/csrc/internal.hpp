@@ -26,13 +26,14 @@ struct rw_tree_im_storage {
   uint32_t sort_tiles = 0;  // tiles per pass at n_cap
 
   void* d_tmp_keys = nullptr;  // [n_cap] ping-pong buffer of the sort
-  uint32_t* d_tree_far = nullptr;  // far lists of the radix tree, then of the octree
+  uint32_t* d_tree_far = nullptr;  // far links of the octree
   uint32_t tree_far_cap = 0;       // entries (16 bytes each)
 
   // zero region
   void* d_zero = nullptr;
   size_t zero_bytes = 0;
   uint32_t* d_ghist = nullptr;      // [passes][radix]
+  uint32_t* d_skew = nullptr;       // [1]: the top sort pass's digits are skewed
   uint32_t* d_sort_desc = nullptr;  // [passes][sort_tiles + 1][radix]
   uint32_t* d_unique_desc = nullptr;
   uint32_t* d_scan_desc = nullptr;
@@ -110,6 +111,10 @@ struct Scratch {
   int passes = 4;
   int sort_variant = 0;
   uint32_t* ghist = nullptr;      // [segments][passes][radix]
+  // [segments]: 1 when the segment's top-pass digits are skewed enough that
+  // ballots rank them faster than shared-memory atomics (k_sort_init sets it,
+  // the kRankMixed variants read it)
+  uint32_t* skew = nullptr;
   uint32_t* sort_desc = nullptr;  // [passes][sort_rows][radix]
   uint32_t sort_rows = 0;         // rows per pass: sort tiles + segments
   uint32_t* unique_desc = nullptr;
@@ -122,8 +127,7 @@ struct Scratch {
   // work only if *gate != 0, read on the device: a fallback sort enqueued
   // ahead of the decision that needs it
   const uint32_t* gate = nullptr;
-  // tree_far_cap entries of 16 bytes: radix-tree gaps left to the far search
-  // (gap, segment: 8 bytes each), then the octree's far links (16 bytes each)
+  // tree_far_cap entries of 16 bytes: the octree's far links
   uint32_t* tree_far = nullptr;
   uint32_t tree_far_cap = 0;
 };

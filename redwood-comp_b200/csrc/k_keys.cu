@@ -119,11 +119,15 @@ __global__ void __launch_bounds__(256)
 // segment's first tile.  Values are absolute positions (segment start added).
 // Descriptor rows of a pass: segment c's init row is toff[c] + c, its tile j
 // uses row toff[c] + c + 1 + j.
+// For the top pass it also sets skew[c] when the digits are skewed: the
+// chance that two keys share a digit, sum over digits of (count / n)^2, above
+// 2^-skew_log2 (many lanes of a warp on one digit then serialise the
+// atomic-OR ranking, which the ballot ranking does not).
 template <int D>
 __global__ void __launch_bounds__(256)
     k_sort_init(const uint32_t* __restrict__ ghist, uint32_t* __restrict__ desc,
                 SegTable seg, TileMap map, int passes, uint32_t rows_per_pass,
-                const uint32_t* __restrict__ gate) {
+                const uint32_t* __restrict__ gate, uint32_t* __restrict__ skew, int skew_log2) {
   pdl_enter();
   if (gate && *gate == 0) return;
   constexpr int RADIX = 1 << D;
@@ -151,6 +155,20 @@ __global__ void __launch_bounds__(256)
     if (first + r < RADIX) row0[first + r] = kFlagInc | (run << 2);
     run += v[r];
   }
+  if (skew && pass == passes - 1) {  // block-uniform
+    __shared__ unsigned long long s_sq[8];
+    unsigned long long sq = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) sq += (unsigned long long)v[r] * v[r];
+    sq = warp_sum(sq);
+    if (lane_id() == 0) s_sq[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long all = 0;
+      for (int w = 0; w < 8; ++w) all += s_sq[w];
+      skew[c] = (all << skew_log2) > (unsigned long long)total * total ? 1u : 0u;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -171,7 +189,7 @@ struct BinCfg {
   // the two-array scheme keeps a match-mask array beside the counters; the
   // half-warp scheme has two words per digit and warp (one per half-warp)
   static constexpr size_t kMatchBytes =
-      (RANK == kRankAtomicOr || RANK == kRankHalfPacked) ? kHistBytes : 0;
+      (RANK == kRankAtomicOr || RANK == kRankHalfPacked || RANK == kRankMixed) ? kHistBytes : 0;
   static constexpr size_t kSmem =
       kKeysBytes + kHistBytes + kMatchBytes + 3 * size_t(RADIX) * 4 + 64 * 4;
   static_assert(kSmem <= 227 * 1024, "onesweep variant exceeds shared memory per CTA");
@@ -185,12 +203,13 @@ struct BinCfg {
 // that a pass that is not needed costs one short wave of CTAs.  A CTA holds a
 // ticket only while it runs, so every look-back still waits only on running
 // tiles, whatever the grid.
-template <typename K, int D, int THREADS, int KPT, int RANK, int MINB, bool PERSIST>
+template <typename K, int D, int THREADS, int KPT, int RANK, int MINB, bool PERSIST, int BB = D>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_binning(const K* __restrict__ in, K* __restrict__ out, SegTable seg, TileMap map,
               int shift, uint32_t* __restrict__ desc,
               uint32_t* __restrict__ tile_ctr, DevStatus* __restrict__ st,
-              uint32_t spin_limit, const uint32_t* __restrict__ gate) {
+              uint32_t spin_limit, const uint32_t* __restrict__ gate,
+              const uint32_t* __restrict__ skew) {
   pdl_enter();
   if (gate && *gate == 0) return;  // every tile of the pass returns: no look-back waits
   using C = BinCfg<K, D, THREADS, KPT, RANK>;
@@ -198,7 +217,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   extern __shared__ __align__(16) unsigned char smem[];
   K* s_keys = reinterpret_cast<K*>(smem);
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem + C::kKeysBytes);
-  uint32_t* s_match = s_hist + NW * RADIX;  // only with kRankAtomicOr
+  uint32_t* s_match = s_hist + NW * RADIX;  // only with kRankAtomicOr / kRankMixed
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + C::kKeysBytes + C::kHistBytes +
                                                 C::kMatchBytes);
   uint32_t* s_start = s_cnt + RADIX;
@@ -212,7 +231,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
       static_assert((NW * RADIX) % 4 == 0 && C::kKeysBytes % 16 == 0, "16-byte zeroing");
       const uint4 z = make_uint4(0, 0, 0, 0);
       constexpr int kWords =
-          (RANK == kRankAtomicOr || RANK == kRankHalfPacked ? 2 : 1) * NW * RADIX;
+          (RANK == kRankAtomicOr || RANK == kRankHalfPacked || RANK == kRankMixed ? 2 : 1) *
+          NW * RADIX;
       for (int i = tid; i < kWords / 4; i += THREADS) reinterpret_cast<uint4*>(s_hist)[i] = z;
     }
     __syncthreads();
@@ -249,17 +269,33 @@ __global__ void __launch_bounds__(THREADS, MINB)
         }
         half_rank<D, KPT, false>(keys, rank2, shift, hbase, n, wp);
       }
+    } else if (RANK == kRankMixed) {
+      // this segment's digits decide the scheme (block-uniform)
+      const bool ballots = skew != nullptr && skew[segc] != 0u;
+      if (full) {
+  #pragma unroll
+        for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
+        warp_rank<D, KPT, kRankMixed, true, BB>(keys, rank2, shift, wbase, n, wh, wm, KPT, ballots);
+      } else {
+  #pragma unroll
+        for (int i = 0; i < KPT; ++i) {
+          const uint32_t idx = wbase + 32u * i;
+          keys[i] = idx < n ? in[idx] : K(0);
+        }
+        warp_rank<D, KPT, kRankMixed, false, BB>(keys, rank2, shift, wbase, n, wh, wm, KPT,
+                                                 ballots);
+      }
     } else if (full) {
   #pragma unroll
       for (int i = 0; i < KPT; ++i) keys[i] = in[wbase + 32u * i];
-      warp_rank<D, KPT, RANK, true>(keys, rank2, shift, wbase, n, wh, wm);
+      warp_rank<D, KPT, RANK, true, BB>(keys, rank2, shift, wbase, n, wh, wm);
     } else {
   #pragma unroll
       for (int i = 0; i < KPT; ++i) {
         const uint32_t idx = wbase + 32u * i;
         keys[i] = idx < n ? in[idx] : K(0);
       }
-      warp_rank<D, KPT, RANK, false>(keys, rank2, shift, wbase, n, wh, wm);
+      warp_rank<D, KPT, RANK, false, BB>(keys, rank2, shift, wbase, n, wh, wm);
     }
     __syncthreads();
 
@@ -422,22 +458,39 @@ cudaError_t keys_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool encode
 }
 
 // probe_spins != 0: the bounded-wait test hook (launch_sort_lookback_probe).
+// RANK kRankMixed: atomic-OR ranking for the passes over full digits; the
+// top pass ranks a segment by ballots over the code's remaining bits when
+// k_sort_init found its top digits skewed (sum of squared digit frequencies
+// above 1/32 for 32-bit keys, 1/64 for 64-bit keys, where the two schemes
+// measured even), else by atomic OR.
 template <typename K, int D, int THREADS, int KPT, int RANK, int MINB>
 cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStream_t s,
                      cudaEvent_t* marks, uint32_t probe_spins) {
-  using C = BinCfg<K, D, THREADS, KPT, RANK>;
+  constexpr int P = (KeyTraits<K>::kCodeBits + D - 1) / D;
+  constexpr int RB = RANK == kRankMixed ? kRankAtomicOr : RANK;  // passes 0 .. P-2
+  constexpr int RT = RANK;                                       // pass P-1
+  constexpr int TB = RANK == kRankMixed ? KeyTraits<K>::kCodeBits - (P - 1) * D : D;
+  constexpr int kSkewLog2 = sizeof(K) == 4 ? 5 : 6;
+  uint32_t* skew = RANK == kRankMixed ? sc.skew : nullptr;
+  using C = BinCfg<K, D, THREADS, KPT, RB>;
+  using CT = BinCfg<K, D, THREADS, KPT, RT>;
   // a gated sort (a fallback that may not be needed) runs persistent passes
   const bool persist = sc.gate != nullptr && !probe_spins;
-  auto kern = persist ? k_binning<K, D, THREADS, KPT, RANK, MINB, true>
-                      : k_binning<K, D, THREADS, KPT, RANK, MINB, false>;
+  auto kern = persist ? k_binning<K, D, THREADS, KPT, RB, MINB, true>
+                      : k_binning<K, D, THREADS, KPT, RB, MINB, false>;
+  auto kern_top = persist ? k_binning<K, D, THREADS, KPT, RT, MINB, true, TB>
+                          : k_binning<K, D, THREADS, KPT, RT, MINB, false, TB>;
   const uint32_t tiles = pl.sort_map.n_tiles;
-  if (tiles + pl.seg.count > sc.sort_rows) return cudaErrorInvalidValue;
+  if (tiles + pl.seg.count > sc.sort_rows || sc.passes != P) return cudaErrorInvalidValue;
   launch_pdl(k_sort_init<D>, pl.seg.count * sc.passes, 256, 0, s, sc.ghist, sc.sort_desc, pl.seg,
-                                                          pl.sort_map, sc.passes, sc.sort_rows, sc.gate);
+             pl.sort_map, sc.passes, sc.sort_rows, sc.gate, skew, kSkewLog2);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], s);
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern_top, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(CT::kSmem));
   if (e != cudaSuccess) return e;
   K* keys = static_cast<K*>(b.keys);
   K* alt = static_cast<K*>(b.alt);
@@ -451,19 +504,21 @@ cudaError_t passes_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
     if (e != cudaSuccess) return e;
     launch_pdl(kern, tiles - 1, THREADS, C::kSmem, s, static_cast<const K*>(keys), alt, pl.seg,
                pl.sort_map, 0, sc.sort_desc, sc.tile_ctr + kCtrSortBase, sc.status,
-               probe_spins, static_cast<const uint32_t*>(nullptr));
+               probe_spins, static_cast<const uint32_t*>(nullptr),
+               static_cast<const uint32_t*>(nullptr));
     return cudaGetLastError();
   }
   const K* src = keys;
   const uint32_t grid =
       persist ? std::min<uint32_t>(tiles, uint32_t(sc.num_sms) * uint32_t(MINB)) : tiles;
-  for (int p = 0; p < sc.passes; ++p) {
-    K* dst = ((sc.passes - 1 - p) % 2 == 0) ? alt : tmp;
+  for (int p = 0; p < P; ++p) {
+    K* dst = ((P - 1 - p) % 2 == 0) ? alt : tmp;
     if (tiles)
-      launch_pdl(kern, grid, THREADS, C::kSmem, s, 
-          src, dst, pl.seg, pl.sort_map, p * D,
-          sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
-          sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit, sc.gate);
+      launch_pdl(p == P - 1 ? kern_top : kern, grid, THREADS, p == P - 1 ? CT::kSmem : C::kSmem,
+                 s, src, dst, pl.seg, pl.sort_map, p * D,
+                 sc.sort_desc + size_t(p) * sc.sort_rows * C::RADIX,
+                 sc.tile_ctr + kCtrSortBase + p, sc.status, sc.spin_limit, sc.gate,
+                 static_cast<const uint32_t*>(p == P - 1 ? skew : nullptr));
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (marks) cudaEventRecord(marks[1 + p], s);
@@ -484,6 +539,7 @@ struct SortVariant {
 // the default).
 const SortVariant kVariants[] = {
     {32, 8, 384, 24, kRankAtomicOr, passes_t<uint32_t, 8, 384, 24, kRankAtomicOr, 3>},
+    {32, 8, 384, 24, kRankMixed, passes_t<uint32_t, 8, 384, 24, kRankMixed, 3>},
     {32, 8, 384, 24, kRankHalfPacked, passes_t<uint32_t, 8, 384, 24, kRankHalfPacked, 3>},
     {32, 8, 512, 16, kRankHalfPacked, passes_t<uint32_t, 8, 512, 16, kRankHalfPacked, 2>},
     {32, 8, 256, 24, kRankHalfPacked, passes_t<uint32_t, 8, 256, 24, kRankHalfPacked, 4>},
@@ -516,6 +572,7 @@ const SortVariant kVariants[] = {
     {32, 11, 256, 16, kRankBallot, passes_t<uint32_t, 11, 256, 16, kRankBallot, 2>},
     {32, 11, 384, 16, kRankBallot, passes_t<uint32_t, 11, 384, 16, kRankBallot, 1>},
     {64, 8, 384, 16, kRankAtomicOr, passes_t<uint64_t, 8, 384, 16, kRankAtomicOr, 2>},
+    {64, 8, 384, 16, kRankMixed, passes_t<uint64_t, 8, 384, 16, kRankMixed, 2>},
     {64, 8, 384, 16, kRankHalfPacked, passes_t<uint64_t, 8, 384, 16, kRankHalfPacked, 2>},
     {64, 8, 256, 16, kRankHalfPacked, passes_t<uint64_t, 8, 256, 16, kRankHalfPacked, 3>},
     {64, 8, 256, 16, kRankAtomicOr, passes_t<uint64_t, 8, 256, 16, kRankAtomicOr, 2>},

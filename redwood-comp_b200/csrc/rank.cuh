@@ -39,7 +39,12 @@ enum RankMode : int {
   kRankBallot = 0,
   kRankMatchAny = 1,
   kRankAtomicOr = 2,
-  kRankHalfPacked = 3  // per half-warp: one word per digit, count << 16 | 16-lane mask
+  kRankHalfPacked = 3,  // per half-warp: one word per digit, count << 16 | 16-lane mask
+  // a sort's mode, not a warp_rank mode: atomic OR for the passes over full
+  // digits, ballots over only the code's remaining bits for the top pass
+  // (skewed top digits put many lanes of a warp on one shared word, which the
+  // atomics serialise; ballots cost the same whatever the digits)
+  kRankMixed = 4
 };
 
 // D ballots, one per digit bit (warp-level multi-split).
@@ -75,11 +80,16 @@ struct RankPack {
 // Stable ranks of one warp's 32*KPT keys among the warp's keys of the same
 // digit (order: step, then lane); the warp's digit counters `wh` advance.
 // FULL: every key is in range, so no per-key checks are made.
-template <int D, int KPT, int RANK, bool FULL, typename K>
+// BB: the digit bits the ballot scheme compares (the bits above them are zero
+// in every key of this pass).
+// RANK kRankMixed: `ballots` (block-uniform) picks the ballot scheme, else
+// the atomic-OR one, per call.
+template <int D, int KPT, int RANK, bool FULL, int BB = D, typename K>
 __device__ __forceinline__ void warp_rank(const K (&keys)[KPT],
                                           uint32_t (&rank2)[RankPack<KPT>::kRegs],
                                           int shift, uint32_t wbase, uint32_t n, uint32_t* wh,
-                                          uint32_t* wm, int steps = KPT) {
+                                          uint32_t* wm, int steps = KPT, bool ballots = false) {
+  const bool by_ballot = RANK == kRankBallot || (RANK == kRankMixed && ballots);
   constexpr uint32_t RADIX = 1u << D;
   const uint32_t lane = lane_id();
 #pragma unroll
@@ -88,8 +98,9 @@ __device__ __forceinline__ void warp_rank(const K (&keys)[KPT],
     const bool valid = FULL || wbase + 32u * i < n;
     const uint32_t dig = uint32_t(keys[i] >> shift) & (RADIX - 1);
     uint32_t peers;
-    if (RANK == kRankBallot) {
-      peers = match_ballot<D>(dig, FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid));
+    static_assert(BB >= 1 && BB <= D, "ballot bits within the digit");
+    if (by_ballot) {
+      peers = match_ballot<BB>(dig, FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid));
     } else if (RANK == kRankMatchAny) {
       peers = __match_any_sync(0xffffffffu, valid ? dig : 0xffffffffu);
       if (!valid) peers = 0;
@@ -104,7 +115,7 @@ __device__ __forceinline__ void warp_rank(const K (&keys)[KPT],
     if (valid && below == 0) {
       // one shared-memory access for the read-modify-write of the counter
       prev = atomicAdd(&wh[dig], uint32_t(__popc(peers)));
-      if (RANK == kRankAtomicOr) wm[dig] = 0;
+      if ((RANK == kRankAtomicOr || RANK == kRankMixed) && !by_ballot) wm[dig] = 0;
     }
     const int leader = valid ? __ffs(peers) - 1 : int(lane);
     prev = __shfl_sync(0xffffffffu, prev, leader);
