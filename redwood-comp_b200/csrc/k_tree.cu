@@ -1296,28 +1296,41 @@ __global__ void __launch_bounds__(256)
   if (count <= far_cap) {
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
          w += gridDim.x * blockDim.x) {
+      // the walk is a chain of dependent loads: every step loads the count,
+      // the parent and the offset of its node together, and the first step
+      // goes out with the segment's counts (k_octree wrote only nodes of the
+      // segment, in [0, n), into the list)
       const uint4 f = reinterpret_cast<const uint4*>(far)[w];
       const uint32_t c = f.x, kind = f.z >> 30, slot = f.z & 7u;
-      const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
-      if (!os.ok) continue;
       const uint32_t sb = seg_begin(seg, c);
       const int32_t* parents = parents_all + sb;
       const int32_t* ec = ec_all + sb;
-      const int n = os.n;
+      const int32_t* off = off_all + sb;
       int rp = int(f.y);
+      const int first = kind != kFarFinal ? parents[rp] : rp;
+      const OctSeg os = oct_segment(seg, o, n_unique, n_octree, seg_err, c, false);
+      if (!os.ok) continue;
+      const int n = os.n;
+      int oct_parent;
       if (kind != kFarFinal) {  // the rest of link_parent's walk
         int counter = int((f.z >> 3) & 31u);
-        rp = parents[rp];
+        rp = first;
         if (uint32_t(rp) >= uint32_t(n)) continue;
         bool stop = kind == kFarFromStep && ++counter > 30;
-        while (!stop && ec[rp] == 0) {
-          rp = parents[rp];
+        int cnt = ec[rp], par = parents[rp];
+        oct_parent = off[rp];
+        while (!stop && cnt == 0) {
+          rp = par;
           if (uint32_t(rp) >= uint32_t(n)) break;
           stop = ++counter > 30;
+          cnt = ec[rp];
+          par = parents[rp];
+          oct_parent = off[rp];
         }
         if (uint32_t(rp) >= uint32_t(n)) continue;
+      } else {
+        oct_parent = off[rp];
       }
-      const int oct_parent = off_all[sb + uint32_t(rp)];
       if (uint32_t(oct_parent) < os.cap) {
         const size_t r = size_t(os.row0) + uint32_t(oct_parent);
         atomicMax(o.children + 8 * r + slot, int32_t(f.w));
