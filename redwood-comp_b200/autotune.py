@@ -2,7 +2,7 @@
 
 For each size class of clouds it times every onesweep variant of the menu
 (threads per CTA, keys per thread, warp ranking scheme) on a synthetic batch of
-that class, for each digit width (8 and 11 bits), and keeps the fastest.  The
+that class, for each digit width (8, 10 and 11 bits), and keeps the fastest.  The
 digit width is one per batch (the digit histograms of every pass are built
 while the keys are encoded), so the width with the smallest summed time wins
 and each class gets its best variant at that width.
