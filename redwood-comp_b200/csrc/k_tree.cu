@@ -434,8 +434,9 @@ struct AnsvCfg {
   static constexpr int VB = sizeof(K) == 4 ? 5 : 6;    // bits of E
   static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
   static constexpr int MW = (kAnsvChunks + 31) / 32;  // mask words per value
-  static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 + 2 * size_t(NV) * kAnsvRow +
-                                  2 * size_t(kTreeTile) + size_t(kAnsvWin) + size_t(kAnsvChunks);
+  static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 + 4 * size_t(kTreeTile) +
+                                  2 * size_t(NV) * kAnsvRow + size_t(kAnsvWin) +
+                                  size_t(kAnsvChunks);
 };
 
 // Warp-cooperative search for the nearest smaller gaps of gap g beyond any
@@ -495,14 +496,12 @@ __device__ void coop_node_keys(const K* __restrict__ codes, int n, int g, int D,
 
 // Writes the node that splits at gap g, given its nearest smaller gaps L, R
 // (see the ANSV comment below); the root (L = -1, R = n) is skipped.
-template <typename K, bool EDGES, typename DAt>
-__device__ __forceinline__ void write_gap_node(int g, int n, int D, int L, int R, const DAt& d_at,
-                                               int root_true_delta, int root_prefix,
-                                               uint8_t* pn, uint8_t* l8, uint8_t* r8,
-                                               int32_t* lcs, int32_t* par, int32_t* ec) {
-  if (L < 0 && R >= n) return;
-  const int dl = L >= 0 ? d_at(L) : -1;
-  const int dr = R < n ? d_at(R) : -1;
+// dl, dr: D of gaps L and R (-1 for the walls at -1 and n).
+template <bool EDGES>
+__device__ __forceinline__ void write_gap_node_d(int g, int D, int L, int R, int dl, int dr,
+                                                 int root_true_delta, int root_prefix,
+                                                 uint8_t* pn, uint8_t* l8, uint8_t* r8,
+                                                 int32_t* lcs, int32_t* par, int32_t* ec) {
   const int i = dr > dl ? R : L + 1;  // left child of R's node, else right child of L's
   const bool leaf_l = g == L + 1, leaf_r = g + 1 == R;
   pn[i] = uint8_t(D);
@@ -516,6 +515,16 @@ __device__ __forceinline__ void write_gap_node(int g, int n, int D, int L, int R
     const int pp = pd == root_true_delta ? root_prefix : pd;
     ec[i] = D / 3 - pp / 3;
   }
+}
+
+template <typename K, bool EDGES, typename DAt>
+__device__ __forceinline__ void write_gap_node(int g, int n, int D, int L, int R, const DAt& d_at,
+                                               int root_true_delta, int root_prefix,
+                                               uint8_t* pn, uint8_t* l8, uint8_t* r8,
+                                               int32_t* lcs, int32_t* par, int32_t* ec) {
+  if (L < 0 && R >= n) return;
+  write_gap_node_d<EDGES>(g, D, L, R, L >= 0 ? d_at(L) : -1, R < n ? d_at(R) : -1,
+                          root_true_delta, root_prefix, pn, l8, r8, lcs, par, ec);
 }
 
 template <typename K, bool EDGES>
@@ -533,11 +542,12 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   // positions inside a chunk are kept as lane indices (0xff: none)
   K* s_key = reinterpret_cast<K*>(smem_raw);                                   // [kAnsvWin + 1]
   uint32_t* s_mask = reinterpret_cast<uint32_t*>(smem_raw + C::kKeyBytes);     // [NV][MW]
-  uint8_t* s_last = reinterpret_cast<uint8_t*>(s_mask + NV * C::MW);           // [NV][kAnsvRow]
+  // the tile's gaps left to phase C: tile index | in-chunk left << 16 |
+  // in-chunk right << 24 (lane indices, 0xff: none)
+  uint32_t* s_pend = s_mask + NV * C::MW;                                      // [kTreeTile]
+  uint8_t* s_last = reinterpret_cast<uint8_t*>(s_pend + kTreeTile);            // [NV][kAnsvRow]
   uint8_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
-  uint8_t* s_lp = s_first + NV * kAnsvRow;                                     // [kTreeTile]
-  uint8_t* s_rp = s_lp + kTreeTile;                                            // [kTreeTile]
-  uint8_t* s_e = s_rp + kTreeTile;                                             // [kAnsvWin]
+  uint8_t* s_e = s_first + NV * kAnsvRow;                                      // [kAnsvWin]
   uint8_t* s_cmin = s_e + kAnsvWin;                                            // [kAnsvChunks]
 
   uint32_t first;
@@ -572,8 +582,11 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   }
 
   __shared__ uint32_t s_far[kTreeFarPerTile];  // the tile's gaps left to phase D
-  __shared__ uint32_t s_far_n;
-  if (threadIdx.x == 0) s_far_n = 0;  // read after the barriers below
+  __shared__ uint32_t s_far_n, s_pend_n;
+  if (threadIdx.x == 0) {  // read after the barriers below
+    s_far_n = 0;
+    s_pend_n = 0;
+  }
 
   // the window's keys [wlo, wlo + kAnsvWin]: one bulk copy when the window
   // lies inside the keys and starts on a 16-byte boundary (every interior
@@ -605,7 +618,10 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   __syncthreads();
 
   // phase A: per chunk, E, the nearest smaller inside the chunk, and the
-  // chunk's summaries (last / first position with E below each value)
+  // chunk's summaries (last / first position with E below each value).  A gap
+  // of the tile whose nearest smaller gaps on both sides lie in its own chunk
+  // (about four in five on uniform keys) writes its node here, with the D of
+  // both from its neighbours' lanes; the others go to the list of phase C.
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   static_assert(C::kKeyBytes % 4 == 0, "the masks follow the keys");
   // two chunks at a time per warp, so that their ballot chains interleave
@@ -654,11 +670,30 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       const uint32_t from0 = __shfl_sync(0xffffffffu, lt0[j], e[j] & 31);
       const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1[j], e[j] & 31) : 0u;
       const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
-      if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {
+      if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {  // warp-uniform
         const int tg = (ch - kAnsvHalo) * 32 + int(lane);
         const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
-        s_lp[tg] = lm ? uint8_t(31 - __clz(lm)) : uint8_t(0xff);
-        s_rp[tg] = rm ? uint8_t(__ffs(rm) - 1) : uint8_t(0xff);
+        const int lp = lm ? 31 - __clz(lm) : -1;
+        const int rp = rm ? __ffs(rm) - 1 : -1;
+        // E of the two nearest smaller lanes (a wall lane past the last gap
+        // has E = 0, so D = -1 there as for the wall at n)
+        const int el = __shfl_sync(0xffffffffu, e[j], lp & 31);
+        const int er = __shfl_sync(0xffffffffu, e[j], rp & 31);
+        const int g = g0 + tg;
+        const bool real = g < n;
+        const bool here = real && lp >= 0 && rp >= 0;
+        if (here)
+          write_gap_node_d<EDGES>(g, e[j] - 1, g - int(lane) + lp, g - int(lane) + rp, el - 1,
+                                  er - 1, root_true_delta, root_prefix, pn, l8, r8, lcs, par,
+                                  EDGES ? edge_count + sb : nullptr);
+        const uint32_t pm = __ballot_sync(0xffffffffu, real && !here);
+        if (pm) {
+          uint32_t at = 0;
+          if (lane == uint32_t(__ffs(pm) - 1)) at = atomicAdd(&s_pend_n, uint32_t(__popc(pm)));
+          at = __shfl_sync(0xffffffffu, at, __ffs(pm) - 1) + __popc(pm & lanemask_lt());
+          if (real && !here)
+            s_pend[at] = uint32_t(tg) | uint32_t(lp & 0xff) << 16 | uint32_t(rp & 0xff) << 24;
+        }
       }
       s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(31 - __clz(lt0[j])) : uint8_t(0xff);
       s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(__ffs(lt0[j]) - 1) : uint8_t(0xff);
@@ -684,21 +719,23 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   }
   __syncthreads();
 
-  // phase C: every gap of the tile writes its node; a gap whose nearest
+  // phase C: every gap of the list writes its node; a gap whose nearest
   // smaller gap lies beyond the window goes to the far-search list
   const int wend = wlo + kAnsvWin - 1;  // last gap of the window
   auto d_at = [&](int p) -> int {       // D of gap p in [0, n)
     return (p >= wlo && p <= wend) ? int(s_e[p - wlo]) - 1 : delta(codes[p], codes[p + 1]);
   };
-  for (int tg = int(threadIdx.x); tg < int(kTreeTile); tg += kTreeThreads) {
+  const int np = int(s_pend_n);
+  for (int q = int(threadIdx.x); q < np; q += kTreeThreads) {
+    const uint32_t pw = s_pend[q];
+    const int tg = int(pw & 0xffffu), lp = int((pw >> 16) & 0xffu), rp = int(pw >> 24);
     const int g = g0 + tg;
-    if (g >= n) break;
     const int ch = kAnsvHalo + tg / 32;
     const int e = s_e[g - wlo];
     // not inside its own chunk: the nearest chunk on that side whose minimum
     // is below e holds the answer in its summary
     const int cb = wlo + ch * 32;  // first gap of this chunk
-    int L = s_lp[tg] != 0xff ? cb + s_lp[tg] : kAnsvNone;
+    int L = lp != 0xff ? cb + lp : kAnsvNone;
     if (L == kAnsvNone) {
       for (int wd = (ch - 1) >> 5; wd >= 0; --wd) {
         uint32_t bits = s_mask[e * C::MW + wd];
@@ -710,7 +747,7 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
         }
       }
     }
-    int R = s_rp[tg] != 0xff ? cb + s_rp[tg] : kAnsvNoneR;
+    int R = rp != 0xff ? cb + rp : kAnsvNoneR;
     if (R == kAnsvNoneR) {
       for (int wd = (ch + 1) >> 5; wd < C::MW; ++wd) {
         uint32_t bits = s_mask[e * C::MW + wd];
@@ -1492,8 +1529,13 @@ cudaError_t tree_t(const Bufs& b, const Scratch& sc, const Plan& pl, bool edges,
   if (!tiles) return cudaSuccess;
   const K* codes = static_cast<const K*>(b.keys);
   constexpr size_t smem = AnsvCfg<K>::kSmem;
-  cudaError_t e = cudaFuncSetAttribute(edges ? k_radix_tree<K, true> : k_radix_tree<K, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const auto kern = edges ? k_radix_tree<K, true> : k_radix_tree<K, false>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  // eight blocks of 32-bit keys need nearly all of the SM's shared memory
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxShared));
   if (e != cudaSuccess) return e;
   if (edges)
     launch_pdl(k_radix_tree<K, true>, tiles, kTreeThreads, smem, s, codes, pl.seg, pl.tree_map,
