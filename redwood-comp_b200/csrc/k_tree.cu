@@ -1038,7 +1038,7 @@ constexpr uint32_t kFarFromParent = 0, kFarFromStep = 1, kFarFinal = 2, kFarLoca
 // sum (k_node_sums, k_tile_scan), the block scans its tile's counts on top
 // of it and writes them to off_all.
 template <typename K, bool OFFS>
-__global__ void __launch_bounds__(kOctThreads)
+__global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bit keys
     k_octree(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
              const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
              int32_t* __restrict__ off_all, const uint32_t* __restrict__ tile_prefix,
@@ -1049,7 +1049,7 @@ __global__ void __launch_bounds__(kOctThreads)
   pdl_enter();
   constexpr int B = KeyTraits<K>::kCodeBits;
   constexpr int kTile = int(kOctTile);
-  constexpr int kRowCap = 2 * kTile;  // rows whose owner is kept
+  constexpr int kRowCap = 3 * kTile / 2;  // rows whose owner is kept
   static_assert(kTile < 0xfff && (kTile & (kTile - 1)) == 0, "12-bit parents, 2^k tile");
   // k = 0 row of each node: child slot values relative to the tile's first
   // row, plus one (0: no child), and the slots taken (one byte per node)
@@ -1559,6 +1559,11 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   // clears its own (a memset between two kernels would also end the
   // programmatic launch chain)
   cudaError_t e = fused_offsets ? cudaSuccess : cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
+  // seven blocks of 32-bit keys need nearly all of the SM's shared memory
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fused_offsets ? k_octree<K, true> : k_octree<K, false>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxShared));
   if (e != cudaSuccess) return e;
   if (tiles) {
     if (fused_offsets)
