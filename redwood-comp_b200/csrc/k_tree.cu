@@ -634,8 +634,9 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       const int w = ch * 32 + int(lane);  // window index of this lane's gap
       const int g = wlo + w;
       const bool real = g >= 0 && g < n;
-      // distinct keys: delta >= 0, so a real gap's E >= 1 and 0 marks walls only
-      e[j] = real ? delta(s_key[w], s_key[w + 1]) + 1 : 0;
+      // distinct keys whose top bit is clear: E = delta + 1 = clz of the xor,
+      // at least 1 for a real gap, so 0 marks walls only
+      e[j] = real ? KeyTraits<K>::clz(s_key[w] ^ s_key[w + 1]) : 0;
       s_e[w] = uint8_t(e[j]);
       const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e[j]));
       if (lane == 0) s_cmin[ch] = uint8_t(cmin);
@@ -1038,7 +1039,7 @@ constexpr uint32_t kFarFromParent = 0, kFarFromStep = 1, kFarFinal = 2, kFarLoca
 // sum (k_node_sums, k_tile_scan), the block scans its tile's counts on top
 // of it and writes them to off_all.
 template <typename K, bool OFFS>
-__global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bit keys
+__global__ void __launch_bounds__(kOctThreads, 8)  // 8 blocks per SM with 32-bit keys
     k_octree(const K* __restrict__ codes_all, const uint8_t* __restrict__ prefix_all,
              const int32_t* __restrict__ parents_all, const int32_t* __restrict__ ec_all,
              int32_t* __restrict__ off_all, const uint32_t* __restrict__ tile_prefix,
@@ -1049,13 +1050,15 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
   pdl_enter();
   constexpr int B = KeyTraits<K>::kCodeBits;
   constexpr int kTile = int(kOctTile);
-  constexpr int kRowCap = 3 * kTile / 2;  // rows whose owner is kept
+  constexpr int kRowCap = kTile;  // rows whose owner is kept
   static_assert(kTile < 0xfff && (kTile & (kTile - 1)) == 0, "12-bit parents, 2^k tile");
   // k = 0 row of each node: child slot values relative to the tile's first
-  // row, plus one (0: no child), and the slots taken (one byte per node)
+  // row, plus one (0: no child; the nonzero slots are the node mask)
   __shared__ uint4 s_child[kTile];  // 8 x u16
-  __shared__ uint32_t s_cmask[kTile / 4];
-  __shared__ int32_t s_off[kTile + 1];  // first row of each node; [kTile]: end of the tile's rows
+  // first row of each node relative to the tile's first row (a tile's rows
+  // number at most kTile times the largest count, 21 levels; 0xffff past the
+  // tile's nodes); [kTile]: end of the tile's rows
+  __shared__ uint16_t s_off[kTile + 2];
   __shared__ K s_code[kTile];
   // per node: (count class << 12) | tile-relative parent (0xfff: outside);
   // class 0: count 0, 1: count > 0, 2: count < 0
@@ -1103,6 +1106,7 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
     s_child[t] = make_uint4(0, 0, 0, 0);
   }
   uint32_t rows_end = 0;
+  int rbase = 0;  // the tile's first row
   if (OFFS) {
     // exclusive scan of the counts in node order, as stage 6 computes it: a
     // warp scan per group of 32 nodes, then one warp scans the 32 group sums
@@ -1122,6 +1126,7 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
     }
     __syncthreads();
     const uint32_t base = tile_prefix[blockIdx.x] - tile_prefix[first];
+    rbase = int(base);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       ov[q] = int32_t(base + s_wsum[q * (kOctThreads / 32) + warp] + inc[q] - uint32_t(ev[q]));
@@ -1129,16 +1134,19 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
       if (i < tile_end) off[i] = ov[q];
     }
     rows_end = base + s_wsum[32];
+  } else {
+    rbase = off[tile0];
   }
   if (!os.ok) return;  // the whole block: no octree row is written
+  // relative rows kept in [0, 0xfffe] (offsets made by stage 6 stay far inside)
+  auto rel16 = [&](int v) -> uint16_t { return uint16_t(min(max(v - rbase, 0), 0xfffe)); };
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int t = tid + q * kOctThreads;
-    s_off[t] = tile0 + t < tile_end ? ov[q] : 0x7fffffff;
+    s_off[t] = tile0 + t < tile_end ? rel16(ov[q]) : uint16_t(0xffff);
   }
-  for (int t = tid; t < kTile / 4; t += kOctThreads) s_cmask[t] = 0;
   if (tid == 0) {
-    s_off[kTile] = OFFS ? int(rows_end) : (tile_end < n ? off[tile_end] : int(m));
+    s_off[kTile] = rel16(OFFS ? int(rows_end) : (tile_end < n ? off[tile_end] : int(m)));
     if (tile0 == 0) {
       const size_t rm = size_t(os.row0) + m;
       int4* row = reinterpret_cast<int4*>(o.children + 8 * rm);
@@ -1158,14 +1166,13 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
   if (tile_end < tile0 + kTile && tid == 0) s_off[tile_end - tile0] = s_off[kTile];
   __syncthreads();
 
-  const int rbase = s_off[0];
-  const int rend = min(s_off[kTile], int(m));  // rows [rbase, rend)
+  const int rend = min(rbase + int(s_off[kTile]), int(m));  // rows [rbase, rend)
   const int root_level = prefix_n[0] / 3;
-  auto owner_of = [&](int p) -> int {  // last node whose first row is <= p
+  auto owner_of = [&](int r) -> int {  // last node whose first row is <= rbase + r
     int t = 0;
 #pragma unroll
     for (int step = kTile / 2; step >= 1; step >>= 1)
-      if (s_off[t + step] <= p) t += step;
+      if (int(s_off[t + step]) <= r) t += step;
     return t;
   };
 
@@ -1178,10 +1185,10 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
   // 16-bit maximum is taken with compare-and-swap on the slot's word.
   for (int r = tid; rbase + r < rend; r += kOctThreads) {
     const int p = rbase + r;
-    const int t = owner_of(p);
+    const int t = owner_of(r);
     if (r < kRowCap) s_owner[r] = uint16_t(t);
-    if (p != s_off[t + 1] - 1) continue;  // not the top row of its chain
-    const int level = int(s_level[t]) - (p - s_off[t]);  // the top row's level
+    if (r != int(s_off[t + 1]) - 1) continue;  // not the top row of its chain
+    const int level = int(s_level[t]) - (r - int(s_off[t]));  // the top row's level
     const int slot = int((s_code[t] >> (B - 3 * level)) & K(7));
     int rp = int(s_node[t] & 0xfffu), counter = 0, x = t;
     uint32_t kind = kFarFromParent;
@@ -1223,10 +1230,7 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
           }
         }
       }
-      if (done) {
-        atomicOr(&s_cmask[rp >> 2], 1u << (slot + 8 * (rp & 3)));
-        continue;
-      }
+      if (done) continue;
       kind = kFarFinal;
     }
     const uint32_t at = atomicAdd(far_n, 1u);
@@ -1242,9 +1246,9 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
   // rows
   for (int r = tid; rbase + r < rend; r += kOctThreads) {
     const int p = rbase + r;
-    const int t = r < kRowCap ? int(s_owner[r]) : owner_of(p);
+    const int t = r < kRowCap ? int(s_owner[r]) : owner_of(r);
     const size_t rp = size_t(os.row0) + uint32_t(p);
-    const int k = p - s_off[t];
+    const int k = r - int(s_off[t]);
     const int level = int(s_level[t]) - k;
     const K code = s_code[t];
     const K pre = code >> (B - 3 * level);
@@ -1258,14 +1262,16 @@ __global__ void __launch_bounds__(kOctThreads, 7)  // 7 blocks per SM with 32-bi
       const uint4 a = s_child[t];
       const uint32_t wv[4] = {a.x, a.y, a.z, a.w};
       int32_t child[8];
+      uint32_t mask = 0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const uint32_t v = (wv[q >> 1] >> (16 * (q & 1))) & 0xffffu;
         child[q] = v ? int32_t(v) - 1 + rbase : 0;
+        mask |= uint32_t(v != 0) << q;
       }
       row[0] = make_int4(child[0], child[1], child[2], child[3]);
       row[1] = make_int4(child[4], child[5], child[6], child[7]);
-      o.node_mask[rp] = int32_t((s_cmask[t >> 2] >> (8 * (t & 3))) & 0xffu);
+      o.node_mask[rp] = int32_t(mask);
     } else {
       int32_t child[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       const int slot = int((code >> (B - 3 * (level + 1))) & K(7));
@@ -1559,7 +1565,7 @@ cudaError_t octree_t(const Bufs& b, const Scratch& sc, const Plan& pl, cudaStrea
   // clears its own (a memset between two kernels would also end the
   // programmatic launch chain)
   cudaError_t e = fused_offsets ? cudaSuccess : cudaMemsetAsync(far_n, 0, sizeof(uint32_t), s);
-  // seven blocks of 32-bit keys need nearly all of the SM's shared memory
+  // eight blocks of 32-bit keys need nearly all of the SM's shared memory
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fused_offsets ? k_octree<K, true> : k_octree<K, false>,
                              cudaFuncAttributePreferredSharedMemoryCarveout,
