@@ -1286,13 +1286,15 @@ __global__ void __launch_bounds__(kOctThreads, 8)  // 8 blocks per SM with 32-bi
 
 // Sum of the edge counts of every tile of kOctTile nodes (the tiles of
 // k_octree), for k_tile_scan: stage 6's reduce on the octree's tiles.  A block
-// takes four tiles, 64 threads and 16 consecutive nodes per thread each.
+// takes four tiles, 64 threads each; thread j of a tile adds the 16-byte
+// vectors j, j + 64, j + 128 and j + 192 of it (a sum needs no order, so the
+// warps read consecutive vectors).
 __global__ void __launch_bounds__(kOctThreads)
     k_node_sums(const int32_t* __restrict__ ec_all, SegTable seg, TileMap map,
                 const uint32_t* __restrict__ n_unique, uint32_t* __restrict__ E) {
   pdl_enter();
-  constexpr int kPer = int(kOctTile) / 64;  // nodes per thread
-  static_assert(kOctThreads == 256 && kPer % 4 == 0, "four tiles of 64 threads");
+  constexpr int kVecs = int(kOctTile) / 4 / 64;  // 16-byte vectors per thread
+  static_assert(kOctThreads == 256 && kVecs * 4 * 64 == int(kOctTile), "four tiles of 64 threads");
   __shared__ uint32_t s_warp[kOctThreads / 32];
   const uint32_t g = threadIdx.x >> 6;  // tile of this thread's group
   const uint32_t tile = 4 * blockIdx.x + g;
@@ -1303,17 +1305,22 @@ __global__ void __launch_bounds__(kOctThreads)
     const uint32_t nu = *reinterpret_cast<const volatile uint32_t*>(n_unique + c);
     const bool ok = nu >= 3 && nu != RW_COUNT_UNSET && nu <= seg_size(seg, c);
     const int n = ok ? int(nu - 1) : 0;
-    const int i0 = int(tile - first) * int(kOctTile) + int(threadIdx.x & 63u) * kPer;
+    const int tb = int(tile - first) * int(kOctTile);
+    const int j = int(threadIdx.x & 63u);
     const int32_t* ec = ec_all + seg_begin(seg, c);
-    if (i0 + kPer <= n && (reinterpret_cast<uintptr_t>(ec + i0) & 15u) == 0) {
+    if (tb + int(kOctTile) <= n && (reinterpret_cast<uintptr_t>(ec + tb) & 15u) == 0) {
+      int4 x[kVecs];
 #pragma unroll
-      for (int q = 0; q < kPer / 4; ++q) {
-        const int4 x = reinterpret_cast<const int4*>(ec + i0)[q];
-        local += uint32_t(x.x) + uint32_t(x.y) + uint32_t(x.z) + uint32_t(x.w);
-      }
+      for (int q = 0; q < kVecs; ++q) x[q] = reinterpret_cast<const int4*>(ec + tb)[q * 64 + j];
+#pragma unroll
+      for (int q = 0; q < kVecs; ++q)
+        local += uint32_t(x[q].x) + uint32_t(x[q].y) + uint32_t(x[q].z) + uint32_t(x[q].w);
     } else {
-      for (int q = 0; q < kPer; ++q)
-        if (i0 + q < n) local += uint32_t(ec[i0 + q]);
+      for (int q = 0; q < kVecs; ++q)
+        for (int e = 0; e < 4; ++e) {
+          const int i = tb + (q * 64 + j) * 4 + e;
+          if (i < n) local += uint32_t(ec[i]);
+        }
     }
   }
   local = warp_sum(local);
