@@ -626,6 +626,12 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   static_assert(C::kKeyBytes % 4 == 0, "the masks follow the keys");
   // two chunks at a time per warp, so that their ballot chains interleave
   static_assert(kAnsvChunks % (2 * NW) == 0, "whole pairs of chunks per warp");
+  // lane v's threshold bits as masks (all ones where v has the bit), the same
+  // for every chunk: kept in registers, since the kernel is bound by its
+  // integer instructions
+  uint32_t mlane[VB];
+#pragma unroll
+  for (int bt = 0; bt < VB; ++bt) mlane[bt] = 0u - ((lane >> bt) & 1u);
   for (int ch0 = int(warp); ch0 < kAnsvChunks; ch0 += 2 * NW) {
     int e[2];
 #pragma unroll
@@ -654,7 +660,8 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       uint32_t B[2];
 #pragma unroll
       for (int j = 0; j < 2; ++j) B[j] = __ballot_sync(0xffffffffu, (e[j] >> bt) & 1);
-      const uint32_t m0 = 0u - ((lane >> bt) & 1u), m1 = 0u - (((lane + 32u) >> bt) & 1u);
+      // v = lane + 32 has bit 5 set and lane's bits below it
+      const uint32_t m0 = mlane[bt], m1 = bt == 5 ? 0xffffffffu : mlane[bt];
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         lt0[j] |= eq0[j] & ~B[j] & m0;
