@@ -639,7 +639,7 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       const int ch = ch0 + j * NW;
       const int w = ch * 32 + int(lane);  // window index of this lane's gap
       const int g = wlo + w;
-      const bool real = g >= 0 && g < n;
+      const bool real = uint32_t(g) < uint32_t(n);
       // distinct keys whose top bit is clear: E = delta + 1 = clz of the xor,
       // at least 1 for a real gap, so 0 marks walls only
       e[j] = real ? KeyTraits<K>::clz(s_key[w] ^ s_key[w + 1]) : 0;
@@ -680,9 +680,10 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
       if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {  // warp-uniform
         const int tg = (ch - kAnsvHalo) * 32 + int(lane);
-        const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lanemask_lt() & ~(1u << lane);
-        const int lp = lm ? 31 - __clz(lm) : -1;
-        const int rp = rm ? __ffs(rm) - 1 : -1;
+        // lt never holds the lane itself; clz(0) = 32 and ffs(0) = 0 give -1
+        const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lm;
+        const int lp = 31 - __clz(lm);
+        const int rp = __ffs(rm) - 1;
         // E of the two nearest smaller lanes (a wall lane past the last gap
         // has E = 0, so D = -1 there as for the wall at n)
         const int el = __shfl_sync(0xffffffffu, e[j], lp & 31);
@@ -703,13 +704,12 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
             s_pend[at] = uint32_t(tg) | uint32_t(lp & 0xff) << 16 | uint32_t(rp & 0xff) << 24;
         }
       }
-      s_last[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(31 - __clz(lt0[j])) : uint8_t(0xff);
-      s_first[int(lane) * kAnsvRow + ch] = lt0[j] ? uint8_t(__ffs(lt0[j]) - 1) : uint8_t(0xff);
+      // an empty mask gives 0xff (none) by itself: 31 - clz(0) = ffs(0) - 1 = -1
+      s_last[int(lane) * kAnsvRow + ch] = uint8_t(31 - __clz(lt0[j]));
+      s_first[int(lane) * kAnsvRow + ch] = uint8_t(__ffs(lt0[j]) - 1);
       if (NV > 32) {
-        s_last[(int(lane) + 32) * kAnsvRow + ch] =
-            lt1[j] ? uint8_t(31 - __clz(lt1[j])) : uint8_t(0xff);
-        s_first[(int(lane) + 32) * kAnsvRow + ch] =
-            lt1[j] ? uint8_t(__ffs(lt1[j]) - 1) : uint8_t(0xff);
+        s_last[(int(lane) + 32) * kAnsvRow + ch] = uint8_t(31 - __clz(lt1[j]));
+        s_first[(int(lane) + 32) * kAnsvRow + ch] = uint8_t(__ffs(lt1[j]) - 1);
       }
     }
   }
