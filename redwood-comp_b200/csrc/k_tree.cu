@@ -424,9 +424,32 @@ struct GlobalKeys {
 constexpr int kAnsvHalo = 8;                                        // chunks per side
 constexpr int kAnsvChunks = int(kTreeTile) / 32 + 2 * kAnsvHalo;   // chunks per window
 constexpr int kAnsvWin = kAnsvChunks * 32;                           // gaps per window
-constexpr int kAnsvRow = kAnsvChunks + 1;  // padded: lane v and chunk c in different banks
+constexpr int kAnsvTileChunks = int(kTreeTile) / 32;
+constexpr int kAnsvRow = kAnsvTileChunks + 1;  // padded: lane v and chunk c in different banks
 constexpr int kAnsvNone = -0x7fffffff;     // "no smaller gap found to the left"
 constexpr int kAnsvNoneR = 0x7fffffff;     // "none to the right"
+
+// Last / first position in a chunk of 32 E values (4-byte aligned) whose
+// value is below e; the caller knows there is one.
+__device__ __forceinline__ int chunk_last_below(const uint8_t* ce, int e) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(ce);
+  const uint32_t ev = 0x01010101u * uint32_t(e);
+  for (int q = 7; q > 0; --q) {
+    const uint32_t below = __vcmpltu4(w[q], ev);  // 0xff in each byte below e
+    if (below) return 4 * q + (31 - __clz(below)) / 8;
+  }
+  return (31 - __clz(__vcmpltu4(w[0], ev))) / 8;
+}
+
+__device__ __forceinline__ int chunk_first_below(const uint8_t* ce, int e) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(ce);
+  const uint32_t ev = 0x01010101u * uint32_t(e);
+  for (int q = 0; q < 7; ++q) {
+    const uint32_t below = __vcmpltu4(w[q], ev);
+    if (below) return 4 * q + (__ffs(below) - 1) / 8;
+  }
+  return 28 + (__ffs(__vcmpltu4(w[7], ev)) - 1) / 8;
+}
 
 template <typename K>
 struct AnsvCfg {
@@ -435,7 +458,7 @@ struct AnsvCfg {
   static constexpr size_t kKeyBytes = (size_t(kAnsvWin) + 1) * sizeof(K);
   static constexpr int MW = (kAnsvChunks + 31) / 32;  // mask words per value
   static constexpr size_t kSmem = kKeyBytes + size_t(NV) * MW * 4 + 4 * size_t(kTreeTile) +
-                                  2 * size_t(NV) * kAnsvRow + size_t(kAnsvWin) +
+                                  size_t(kAnsvWin) + 2 * size_t(NV) * kAnsvRow +
                                   size_t(kAnsvChunks);
 };
 
@@ -545,10 +568,11 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   // the tile's gaps left to phase C: tile index | in-chunk left << 16 |
   // in-chunk right << 24 (lane indices, 0xff: none)
   uint32_t* s_pend = s_mask + NV * C::MW;                                      // [kTreeTile]
-  uint8_t* s_last = reinterpret_cast<uint8_t*>(s_pend + kTreeTile);            // [NV][kAnsvRow]
+  uint8_t* s_e = reinterpret_cast<uint8_t*>(s_pend + kTreeTile);               // [kAnsvWin]
+  // summaries of the tile's chunks only (a halo chunk is scanned when asked)
+  uint8_t* s_last = s_e + kAnsvWin;                                            // [NV][kAnsvRow]
   uint8_t* s_first = s_last + NV * kAnsvRow;                                   // [NV][kAnsvRow]
-  uint8_t* s_e = s_first + NV * kAnsvRow;                                      // [kAnsvWin]
-  uint8_t* s_cmin = s_e + kAnsvWin;                                            // [kAnsvChunks]
+  uint8_t* s_cmin = s_first + NV * kAnsvRow;                                   // [kAnsvChunks]
 
   uint32_t first;
   const uint32_t c = tile_segment(seg, map, blockIdx.x, &first);
@@ -624,15 +648,28 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
   // both from its neighbours' lanes; the others go to the list of phase C.
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   static_assert(C::kKeyBytes % 4 == 0, "the masks follow the keys");
-  // two chunks at a time per warp, so that their ballot chains interleave
-  static_assert(kAnsvChunks % (2 * NW) == 0, "whole pairs of chunks per warp");
+  // the halo chunks need only E and their minimum: a lookup that ends in one
+  // scans its 32 values (phase C)
+  static_assert(2 * kAnsvHalo % NW == 0, "whole rounds of halo chunks");
+  for (int hc = int(warp); hc < 2 * kAnsvHalo; hc += NW) {
+    const int ch = hc < kAnsvHalo ? hc : hc + kAnsvTileChunks;
+    const int w = ch * 32 + int(lane);
+    const int g = wlo + w;
+    const int e = uint32_t(g) < uint32_t(n) ? KeyTraits<K>::clz(s_key[w] ^ s_key[w + 1]) : 0;
+    s_e[w] = uint8_t(e);
+    const uint32_t cmin = __reduce_min_sync(0xffffffffu, uint32_t(e));
+    if (lane == 0) s_cmin[ch] = uint8_t(cmin);
+  }
+  // the tile's chunks two at a time per warp, so that their ballot chains
+  // interleave
+  static_assert(kAnsvTileChunks % (2 * NW) == 0, "whole pairs of chunks per warp");
   // lane v's threshold bits as masks (all ones where v has the bit), the same
   // for every chunk: kept in registers, since the kernel is bound by its
   // integer instructions
   uint32_t mlane[VB];
 #pragma unroll
   for (int bt = 0; bt < VB; ++bt) mlane[bt] = 0u - ((lane >> bt) & 1u);
-  for (int ch0 = int(warp); ch0 < kAnsvChunks; ch0 += 2 * NW) {
+  for (int ch0 = kAnsvHalo + int(warp); ch0 < kAnsvHalo + kAnsvTileChunks; ch0 += 2 * NW) {
     int e[2];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -678,7 +715,7 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
       const uint32_t from0 = __shfl_sync(0xffffffffu, lt0[j], e[j] & 31);
       const uint32_t from1 = NV > 32 ? __shfl_sync(0xffffffffu, lt1[j], e[j] & 31) : 0u;
       const uint32_t lt = (NV > 32 && e[j] >= 32) ? from1 : from0;
-      if (ch >= kAnsvHalo && ch < kAnsvHalo + int(kTreeTile) / 32) {  // warp-uniform
+      {
         const int tg = (ch - kAnsvHalo) * 32 + int(lane);
         // lt never holds the lane itself; clz(0) = 32 and ffs(0) = 0 give -1
         const uint32_t lm = lt & lanemask_lt(), rm = lt & ~lm;
@@ -705,11 +742,12 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
         }
       }
       // an empty mask gives 0xff (none) by itself: 31 - clz(0) = ffs(0) - 1 = -1
-      s_last[int(lane) * kAnsvRow + ch] = uint8_t(31 - __clz(lt0[j]));
-      s_first[int(lane) * kAnsvRow + ch] = uint8_t(__ffs(lt0[j]) - 1);
+      const int tc = ch - kAnsvHalo;  // the chunk's column among the tile's
+      s_last[int(lane) * kAnsvRow + tc] = uint8_t(31 - __clz(lt0[j]));
+      s_first[int(lane) * kAnsvRow + tc] = uint8_t(__ffs(lt0[j]) - 1);
       if (NV > 32) {
-        s_last[(int(lane) + 32) * kAnsvRow + ch] = uint8_t(31 - __clz(lt1[j]));
-        s_first[(int(lane) + 32) * kAnsvRow + ch] = uint8_t(__ffs(lt1[j]) - 1);
+        s_last[(int(lane) + 32) * kAnsvRow + tc] = uint8_t(31 - __clz(lt1[j]));
+        s_first[(int(lane) + 32) * kAnsvRow + tc] = uint8_t(__ffs(lt1[j]) - 1);
       }
     }
   }
@@ -750,7 +788,8 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
         if (wd == (ch - 1) >> 5) bits &= 0xffffffffu >> (31 - ((ch - 1) & 31));
         if (bits) {
           const int c2 = wd * 32 + 31 - __clz(bits);
-          L = wlo + c2 * 32 + s_last[e * kAnsvRow + c2];
+          L = wlo + c2 * 32 + (c2 >= kAnsvHalo ? int(s_last[e * kAnsvRow + c2 - kAnsvHalo])
+                                               : chunk_last_below(s_e + c2 * 32, e));
           break;
         }
       }
@@ -762,7 +801,9 @@ __global__ void __launch_bounds__(kTreeThreads, 8)  // 8 blocks (64 warps) per S
         if (wd == (ch + 1) >> 5) bits &= 0xffffffffu << ((ch + 1) & 31);
         if (bits) {
           const int c2 = wd * 32 + __ffs(bits) - 1;
-          R = wlo + c2 * 32 + s_first[e * kAnsvRow + c2];
+          R = wlo + c2 * 32 +
+              (c2 < kAnsvHalo + kAnsvTileChunks ? int(s_first[e * kAnsvRow + c2 - kAnsvHalo])
+                                                : chunk_first_below(s_e + c2 * 32, e));
           break;
         }
       }
