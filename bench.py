@@ -120,17 +120,74 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    NVML's read-only clock and clock-event-reason queries, from a thread, about
+    every millisecond while the region runs, so that a region of a few
+    milliseconds still has samples under load; the region starts after the
+    first sample.  Without NVML: nvidia-smi every 200 ms around the region."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    # NVML clock-event-reason bits (nvml.h nvmlClocksEventReason*)
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+                   ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.001):
         self.gpu = gpu_index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.samples = []
+        self.lines = []
+
+    def _nvml_handle(self, nv):
+        """The NVML device of this process's CUDA device: by PCI address when
+        torch reports it (CUDA ordinals and NVML indices differ under
+        CUDA_VISIBLE_DEVICES), else by index."""
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(torch.cuda.current_device())
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus), "pci"
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu), "index"
+
+    def _loop(self):
+        nv = self.nvml
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                self.first.set()
+                return
+            self.samples.append((float(sm), int(rs)))
+            self.first.set()
+            if self.stop.wait(self.period):
+                return
 
     def __enter__(self):
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nvml = nv
+            self.h, self.match = self._nvml_handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self.stop, self.first = threading.Event(), threading.Event()
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
+            self.first.wait(1.0)
+            return self
+        except Exception:
+            if self.nvml is not None:
+                try:
+                    self.nvml.nvmlShutdown()
+                except Exception:
+                    pass
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -142,7 +199,14 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self.nvml is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return False
         if self.proc is None:
             return False
         time.sleep(0.25)
@@ -156,7 +220,15 @@ class ClockSampler:
         return False
 
     def summary(self):
-        if not getattr(self, "lines", None):
+        if self.samples:
+            sm = [x for x, _ in self.samples]
+            reasons = sorted({nm for _, rs in self.samples for nm, bit in self.REASON_BITS
+                              if rs & bit})
+            return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm),
+                    "sm_max_mhz": self.max_mhz, "samples": len(sm), "reasons": reasons,
+                    "source": f"nvml every {self.period * 1e3:g} ms inside the timed region "
+                              f"(device by {self.match})"}
+        if not self.lines:
             return None
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -173,7 +245,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "samples": len(sm),
-                "reasons": sorted(reasons)}
+                "reasons": sorted(reasons), "source": "nvidia-smi every 200 ms around the region"}
 
 
 def kernel_bytes(name, n, u, m, K):

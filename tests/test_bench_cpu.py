@@ -118,3 +118,50 @@ def test_two_ranks_take_the_slowest_step():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert out[0] == out[1] == 4.25
+
+
+def test_clock_sampler_reads_nvml_inside_the_region(monkeypatch):
+    """The clock sampler takes NVML samples from a thread while the timed region
+    runs (read-only queries: clock, max clock, clock-event reasons) and reports
+    the median, the sample count and every throttle reason seen.  A fake NVML
+    module stands in for the driver; a region with a power-capped sample
+    reports sw_power_cap."""
+    import time
+
+    state = {"calls": 0, "shut": False}
+
+    class FakeNvml(types.ModuleType):
+        NVML_CLOCK_SM = 1
+
+        def nvmlInit(self):
+            pass
+
+        def nvmlShutdown(self):
+            state["shut"] = True
+
+        def nvmlDeviceGetHandleByPciBusId(self, bus):
+            raise RuntimeError("no PCI address here")
+
+        def nvmlDeviceGetHandleByIndex(self, i):
+            return ("dev", i)
+
+        def nvmlDeviceGetMaxClockInfo(self, h, kind):
+            return 1965
+
+        def nvmlDeviceGetClockInfo(self, h, kind):
+            state["calls"] += 1
+            return 1965 if state["calls"] % 2 else 1950
+
+        def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+            return 0x4 if state["calls"] == 3 else 0
+
+    monkeypatch.setitem(sys.modules, "pynvml", FakeNvml("pynvml"))
+    bench = load_bench()
+    with bench.ClockSampler(0, period_s=0.001) as c:
+        time.sleep(0.05)
+    s = c.summary()
+    assert state["shut"]
+    assert s["samples"] >= 5 and s["samples"] == state["calls"]
+    assert s["sm_max_mhz"] == 1965.0 and s["sm_mhz"] in (1950.0, 1957.5, 1965.0)
+    assert s["reasons"] == ["sw_power_cap"]
+    assert "nvml" in s["source"] and "index" in s["source"]
