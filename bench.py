@@ -56,6 +56,9 @@ def parse_args():
                    help="onesweep variant index (default: the storage's default)")
     p.add_argument("--only-device", action="store_true",
                    help="time only the device-resident pipeline (for profiler runs)")
+    p.add_argument("--slots", type=int, default=2,
+                   help="clouds in flight in the device-resident timed region (AppData / "
+                        "scratch pairs on their own streams, steps taken in turn)")
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batched and learned forms in the default line")
     # internal: time the reference's CPU path in a child process (see ref_time_isolated)
@@ -852,6 +855,61 @@ def main():
                               "mismatches_vs_oracle": mismatches}), flush=True)
         return 0
 
+    # ---- several clouds in flight --------------------------------------------
+    # More AppData / scratch pairs, each on its own stream, the K timed steps
+    # taken by the pairs in turn (the same cloud, the same seven stages each
+    # step): one cloud's kernels with few blocks (the one-block tile scans, the
+    # sort set-up, the octree's far links) and every kernel's ramp-up and tail
+    # then overlap another cloud's kernels, as consecutive clouds of a stream of
+    # clouds can.  `value` is this throughput; `one_stream` is the region
+    # above, one cloud after another on one stream.
+    one_stream_ms = ms_step
+    inflight = max(1, a.slots)
+    extra = []
+    for _ in range(inflight - 1):
+        app_k = rw.AppData(a.n, a.key_bits, points=pts)
+        im_k = rw.ImStorage(a.n, a.key_bits, a.radix_bits)
+        if a.sort_variant >= 0:
+            im_k.set_sort_variant(a.sort_variant)
+        extra.append((app_k, im_k, torch.cuda.Stream()))
+    for app_k, im_k, s_k in extra:
+        for _ in range(a.warmup):
+            rw.run_pipeline(app_k, im_k, s_k)
+    torch.cuda.synchronize()
+    slot_mismatches = None
+    if mismatches is not None:
+        slot_mismatches = 0
+        for app_k, _, _ in extra:
+            got_k = app_k.results()
+            slot_mismatches += sum(
+                1 for k, v in want.items()
+                if (np.ascontiguousarray(got_k[k]).tobytes() != np.ascontiguousarray(v).tobytes()
+                    if isinstance(v, np.ndarray) else got_k[k] != v))
+    pairs = [(app, im, stream)] + extra
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks_k:
+        ev2.record(stream)
+        for _, _, s_k in extra:
+            s_k.wait_stream(stream)
+        for i in range(a.steps):
+            app_k, im_k, s_k = pairs[i % inflight]
+            rw.pipeline_enqueue(app_k, im_k, s_k)
+        for _, _, s_k in extra:
+            stream.wait_stream(s_k)
+        ev3.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    for app_k, im_k, s_k in pairs:
+        rw.pipeline_finish(app_k, im_k, s_k)
+    ms_step = max_over_ranks(ev2.elapsed_time(ev3) / a.steps)
+    value = a.n * world / (ms_step / 1e3)
+    one_stream = {"value": a.n * world / (one_stream_ms / 1e3), "ms_per_step": one_stream_ms,
+                  "clocks": clocks.summary()}
+    clocks = clocks_k
+    del extra, pairs
+
     # ---- per-kernel device times inside the pipeline -----------------------
     kms = rw.profile_pipeline(app, im, reps=max(3, min(10, a.steps)))
     hbm, peak_kind = peaks()
@@ -989,6 +1047,8 @@ def main():
         "dtype": f"u{a.key_bits}", "data": "synthetic",
         "config": config_of(a),
         "n_unique": u, "n_octree_nodes": m, "mismatches_vs_oracle": mismatches,
+        "slots": inflight, "other_slots_mismatches_vs_oracle": slot_mismatches,
+        "one_stream": one_stream,
         "pipeline_roofline": {"bytes_per_step": pipe_b, "achieved_gbs": round(pipe_gbs, 1),
                               "frac": round(pipe_gbs / hbm, 4)},
         "roofline": roofline, "stages": stages, "e2e": e2e, "cpu_baseline": cpu,
