@@ -121,6 +121,29 @@ def test_buffers_reused_across_inputs(rw, oracle):
     assert_same(app.results(), oracle.run(a), "reuse stagewise")
 
 
+def test_two_clouds_in_flight_on_two_streams(rw, oracle):
+    """Two AppData/ImStorage pairs on two streams, their pipelines enqueued in
+    turn with no host wait in between (how a stream of clouds keeps two in
+    flight, as bench.py's device-resident region does): each pair ends with the
+    oracle's outputs for its own cloud, so scratch sets share no device state."""
+    import torch
+    n = 300000
+    pts = [cloud(rw, n, "uniform", 31), cloud(rw, n, "gauss", 32)]
+    pairs = [(rw.AppData(n, 32, points=p), rw.ImStorage(n, 32), torch.cuda.Stream())
+             for p in pts]
+    torch.cuda.synchronize()
+    for app, im, s in pairs:
+        rw.run_pipeline(app, im, s)
+    torch.cuda.synchronize()
+    for i in range(6):
+        app, im, s = pairs[i % 2]
+        rw.pipeline_enqueue(app, im, s)
+    for app, im, s in pairs:
+        rw.pipeline_finish(app, im, s)
+    for k, ((app, _, _), p) in enumerate(zip(pairs, pts)):
+        assert_same(app.results(), oracle.run(p), f"pair {k} of two in flight")
+
+
 def test_pipeline_replayed_from_a_cuda_graph(rw, oracle):
     """rw_tree_pipeline_enqueue captured once into a CUDA graph (the kernels use
     programmatic dependent launch) and replayed on new clouds in the same
