@@ -59,6 +59,8 @@ def parse_args():
     p.add_argument("--slots", type=int, default=2,
                    help="clouds in flight in the device-resident timed region (AppData / "
                         "scratch pairs on their own streams, steps taken in turn)")
+    p.add_argument("--e2e-slots", type=int, default=3,
+                   help="AppData / scratch pairs and streams of the end-to-end region")
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batched and learned forms in the default line")
     # internal: time the reference's CPU path in a child process (see ref_time_isolated)
@@ -963,7 +965,7 @@ def main():
     # copy in of cloud k does not wait behind the copy out of the cloud before
     # it on the same stream while another cloud's copy out holds the
     # device-to-host direction
-    n_slots = 3
+    n_slots = max(2, a.e2e_slots)
     slots = [(app, im, torch.cuda.Stream(), outs_np)]
     for _ in range(n_slots - 1):
         ax = rw.AppData(a.n, a.key_bits, points=pts)
@@ -1008,9 +1010,9 @@ def main():
            "copy_floor_note": "the same step's copies alone (points host to device on one "
                               "stream, the five octree arrays device to host on another, "
                               "pinned buffers, no kernels), the PCIe bound of this number",
-           "path": "rw_tree_host_submit / rw_tree_host_collect on three AppData/scratch "
-                   "pairs and three streams: pinned host points -> H2D -> 7 stages -> counts + "
-                   "octree rows (children, corner, cell_size, masks) D2H, every step"}
+           "path": f"rw_tree_host_submit / rw_tree_host_collect on {n_slots} AppData/scratch "
+                   f"pairs and {n_slots} streams: pinned host points -> H2D -> 7 stages -> "
+                   "counts + octree rows (children, corner, cell_size, masks) D2H, every step"}
     del slots[1:]
 
     cpu = None
